@@ -1,0 +1,296 @@
+/*
+ * dcfr.h — C ABI of libdcfr, the B200 heads-up Discounted-CFR range-vs-range
+ * postflop solver.
+ *
+ * The ABI mirrors the public API of the reference solver crate
+ * (AhanDatta/Poker-Trainer, crates/solver/src/lib.rs): build a game from a
+ * board, two 1326-combo ranges, a root betting state and bet menus; solve it
+ * with DCFR; query per-node strategies, EVs, ranges and exploitability.
+ * Every function returns an int status (DCFR_OK or a DCFR_ERR_* code); the
+ * message of the last failure on the calling thread is dcfr_last_error().
+ * All buffers are caller-allocated. There is no CPU fallback: a solver
+ * handle owns one CUDA stream on the current device, and every iteration,
+ * best response and query traversal runs in the library's sm_100a kernels.
+ * One handle is used by one thread at a time.
+ *
+ * Card ids are rank*4+suit with ranks 2..A = 0..12 and suits c,d,h,s = 0..3
+ * (crates/holdem/src/card.rs:46). Combo ids are hi*(hi-1)/2+lo over card ids
+ * with hi > lo (crates/holdem/src/combo.rs:14-17).
+ */
+#ifndef DCFR_H
+#define DCFR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DCFR_NUM_COMBOS 1326
+#define DCFR_MAX_SIZES 8
+
+/* Status codes. The first four mirror SolverError
+ * (crates/solver/src/lib.rs:186-192). */
+enum {
+  DCFR_OK = 0,
+  DCFR_ERR_EMPTY_RANGE = 1,   /* SolverError::EmptyRange(player) */
+  DCFR_ERR_INVALID_BOARD = 2, /* SolverError::InvalidBoard */
+  DCFR_ERR_TOO_LARGE = 3,     /* SolverError::TooLarge{needed, limit} */
+  DCFR_ERR_BAD_PATH = 4,      /* SolverError::BadPath */
+  DCFR_ERR_INVALID_ARG = 5,   /* malformed config, NULL pointer, short buffer */
+  DCFR_ERR_CUDA = 6,          /* a CUDA runtime call failed */
+  DCFR_ERR_OUT_OF_MEMORY = 7, /* device memory exhausted */
+  DCFR_ERR_UNSUPPORTED = 8,   /* option not built (e.g. sampled chance) */
+  DCFR_ERR_DEVICE_TIMEOUT = 9 /* a bounded device-side wait gave up */
+};
+
+/* Streets (holdem::Street, crates/holdem/src/game.rs:19-25). */
+enum { DCFR_PREFLOP = 0, DCFR_FLOP = 1, DCFR_TURN = 2, DCFR_RIVER = 3 };
+
+/* Bet size kinds (holdem::menu::BetSize, crates/holdem/src/menu.rs:16-24). */
+enum { DCFR_SIZE_POT = 0, DCFR_SIZE_MULT = 1, DCFR_SIZE_ALLIN = 2 };
+
+/* Action kinds (holdem::Action, crates/holdem/src/game.rs:76-82). */
+enum { DCFR_FOLD = 0, DCFR_CHECK = 1, DCFR_CALL = 2, DCFR_RAISE = 3 };
+
+/* Storage modes (StorageMode, crates/solver/src/storage.rs:79-85). */
+enum { DCFR_STORAGE_F32 = 0, DCFR_STORAGE_COMPRESSED = 1, DCFR_STORAGE_AUTO = 2 };
+
+/* Traversal modes (cfr::Mode, crates/solver/src/cfr.rs:248-256). */
+enum { DCFR_MODE_CFR = 0, DCFR_MODE_BEST_RESPONSE = 1, DCFR_MODE_AVERAGE = 2 };
+
+/* One bet size: kind DCFR_SIZE_*, value = pot fraction (0.75 for 75%) or
+ * raise multiple (3.0 for 3x); ignored for all-in. */
+typedef struct dcfr_bet_size {
+  int32_t kind;
+  int32_t _pad;
+  double value;
+} dcfr_bet_size;
+
+/* StreetSizes (crates/holdem/src/menu.rs:87-91). */
+typedef struct dcfr_street_sizes {
+  int32_t n_bet;
+  int32_t n_raise;
+  dcfr_bet_size bet[DCFR_MAX_SIZES];
+  dcfr_bet_size raise[DCFR_MAX_SIZES];
+} dcfr_street_sizes;
+
+/* PostflopMenu (crates/holdem/src/menu.rs:102-117). */
+typedef struct dcfr_menu {
+  dcfr_street_sizes flop;
+  dcfr_street_sizes turn;
+  dcfr_street_sizes river;
+  uint32_t max_raises;
+  uint32_t _pad;
+  double add_allin_threshold;
+  double force_allin_threshold;
+  double merge_threshold;
+} dcfr_menu;
+
+/* BettingState (crates/solver/src/tree.rs:19-34). Player 0 is out of
+ * position. */
+typedef struct dcfr_betting_state {
+  int32_t street;
+  int32_t to_act;
+  int64_t pot;
+  int64_t commit[2];
+  int64_t stack[2];
+  int64_t current_bet;
+  int64_t last_raise_inc;
+  uint32_t num_raises;
+  uint8_t needs[2];
+  uint8_t _pad[2];
+} dcfr_betting_state;
+
+/* DcfrParams (crates/solver/src/cfr.rs:48-63). beta_clip != 0 means
+ * beta = None (negative regrets clipped to zero, DCFR+). */
+typedef struct dcfr_params {
+  double alpha;
+  double beta;
+  double gamma;
+  int32_t beta_clip;
+  int32_t restart_average;
+  int32_t unweighted_average;
+  int32_t _pad;
+} dcfr_params;
+
+/* SolveConfig (crates/solver/src/lib.rs:74-105). Ranges are inline
+ * 1326-entry weight vectors indexed by combo id. keep[p] lists up to
+ * n_keep[p] combo ids that pruning must never drop. */
+typedef struct dcfr_config {
+  uint8_t board[5];
+  uint8_t _pad0[3];
+  int32_t board_len;
+  int32_t _pad1;
+  float ranges[2][DCFR_NUM_COMBOS];
+  dcfr_betting_state root;
+  dcfr_menu menu;
+  int32_t has_future_menu;
+  int32_t _pad2;
+  dcfr_menu future_menu;
+  int64_t big_blind;
+  float prune;
+  int32_t n_keep[2];
+  int32_t _pad3;
+  uint16_t keep[2][DCFR_NUM_COMBOS];
+  uint64_t max_memory_bytes;
+  double rake_rate;
+  double rake_cap;
+  int32_t storage;
+  int32_t isomorphism;
+  dcfr_params dcfr;
+} dcfr_config;
+
+/* TreeStats (crates/solver/src/tree.rs:248-257). */
+typedef struct dcfr_tree_stats {
+  uint64_t player_nodes;
+  uint64_t chance_nodes;
+  uint64_t terminal_nodes;
+  uint64_t storage_cells;
+  int32_t compressed;
+  int32_t _pad;
+  uint64_t memory_bytes;
+} dcfr_tree_stats;
+
+/* SolveOptions (crates/solver/src/lib.rs:137-147). */
+typedef struct dcfr_solve_options {
+  uint32_t max_iterations;
+  uint32_t check_every;
+  double target_exploitability_pct;
+} dcfr_solve_options;
+
+/* Progress (crates/solver/src/lib.rs:174-184). */
+typedef struct dcfr_progress {
+  uint32_t iteration;
+  uint32_t max_iterations;
+  double exploitability;
+  double exploitability_pct;
+  int32_t finished;
+  int32_t _pad;
+} dcfr_progress;
+
+/* Called after every exploitability check; returning 0 cancels the solve
+ * (the on_progress closure of Solver::solve, lib.rs:475). */
+typedef int (*dcfr_progress_cb)(const dcfr_progress* progress, void* user);
+
+/* A path step (Step, crates/solver/src/lib.rs:212-217): kind 0 = action
+ * (action_kind DCFR_FOLD..DCFR_RAISE, amount = raise-to chips), kind 1 =
+ * dealt card. */
+typedef struct dcfr_step {
+  int32_t kind;
+  int32_t action_kind;
+  int64_t amount;
+  uint8_t card;
+  uint8_t _pad[7];
+} dcfr_step;
+
+typedef struct dcfr_action {
+  int32_t kind;
+  int32_t _pad;
+  int64_t amount;
+} dcfr_action;
+
+/* Header of NodeInfo (crates/solver/src/lib.rs:220-240); the arrays are
+ * written by dcfr_query into caller buffers sized from dcfr_query_sizes. */
+typedef struct dcfr_node_info {
+  int32_t player;
+  int32_t num_actions;
+  int32_t num_hands;
+  int32_t _pad;
+  double reach_fraction[2];
+  int64_t pot;
+  int64_t invest[2];
+} dcfr_node_info;
+
+typedef struct dcfr_solver dcfr_solver;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* dcfr_last_error(void);
+
+/* SolveConfig::new defaults (lib.rs:110-134) with the default PostflopMenu
+ * (menu.rs:119-133): exact runouts, no rake, Auto storage, isomorphism on,
+ * 8 GiB limit, DcfrParams::default (cfr.rs:72-80). board/ranges/root are
+ * left zeroed for the caller. */
+int dcfr_config_init(dcfr_config* cfg);
+
+/* Solver::estimate (lib.rs:355-362): tree size without building it. */
+int dcfr_estimate(const dcfr_config* cfg, dcfr_tree_stats* out);
+
+/* Solver::new (lib.rs:365-396): builds the tree, the strength tables and
+ * the device plan, and allocates device storage on the current device. */
+int dcfr_create(const dcfr_config* cfg, dcfr_solver** out);
+void dcfr_destroy(dcfr_solver* s);
+
+/* Solver::solve_cancellable (lib.rs:482-494) over run_solve
+ * (lib.rs:594-642): iterations, exploitability checks on the
+ * next_check_gap schedule (lib.rs:158-172), cancellation checked before
+ * every iteration. cancel and cb may be NULL. */
+int dcfr_solve(dcfr_solver* s, const dcfr_solve_options* opts, const volatile int32_t* cancel,
+               dcfr_progress_cb cb, void* user, dcfr_progress* out);
+
+/* Runs exactly n DCFR iterations (cpu_iteration, lib.rs:577-585) with no
+ * exploitability checks. Asynchronous on the handle's stream. */
+int dcfr_iterate(dcfr_solver* s, uint32_t n);
+/* Waits for the handle's stream. */
+int dcfr_synchronize(dcfr_solver* s);
+
+/* Solver::exploitability (lib.rs:462-464), chips. */
+int dcfr_exploitability(dcfr_solver* s, double* out);
+/* Solver::root_values (lib.rs:468-470): average-strategy EV of each player. */
+int dcfr_root_values(dcfr_solver* s, double out[2]);
+/* Solver::iterations, last_exploitability, stats, root_pot. */
+int dcfr_iterations(const dcfr_solver* s, uint32_t* out);
+int dcfr_last_exploitability(const dcfr_solver* s, double* out);
+int dcfr_stats(const dcfr_solver* s, dcfr_tree_stats* out);
+/* Number of suit pairs solved through isomorphism (lib.rs:416-418). */
+int dcfr_isomorphic_pairs(const dcfr_solver* s, int32_t* out);
+
+/* Solver::hands (hands.rs:15-30): number of hands of player p, and their
+ * combo ids and root weights (either pointer may be NULL). */
+int dcfr_hands(const dcfr_solver* s, int32_t p, uint16_t* combos, float* weights, int32_t* n);
+
+/* Solver::is_decision / actions_at / query / ranges_after
+ * (lib.rs:828-912). dcfr_query_sizes gives the array sizes of dcfr_query:
+ * actions[num_actions], combos[num_hands], strategy/ev[num_actions*num_hands]
+ * (action-major), reach[num_hands]. */
+int dcfr_is_decision(dcfr_solver* s, const dcfr_step* path, size_t n, int32_t* out);
+int dcfr_actions_at(dcfr_solver* s, const dcfr_step* path, size_t n, dcfr_action* actions, size_t cap,
+                    size_t* count);
+int dcfr_query_sizes(dcfr_solver* s, const dcfr_step* path, size_t n, int32_t* num_actions,
+                     int32_t* num_hands);
+int dcfr_query(dcfr_solver* s, const dcfr_step* path, size_t n, dcfr_node_info* info,
+               dcfr_action* actions, uint16_t* combos, float* strategy, float* ev, float* reach);
+int dcfr_ranges_after(dcfr_solver* s, const dcfr_step* path, size_t n, float out[2][DCFR_NUM_COMBOS]);
+
+/* Storage in the reference layout (storage.rs:87-98; one action-major
+ * block per decision node at Node::offset, tree.rs:200-204): len f32
+ * regrets and len f32 strategy sums. Used to resume a solve elsewhere
+ * (lib.rs:532-540) and by the parity tests. */
+int dcfr_storage_len(const dcfr_solver* s, uint64_t* len);
+int dcfr_download_storage(dcfr_solver* s, float* regrets, float* sums, uint64_t len);
+int dcfr_upload_storage(dcfr_solver* s, const float* regrets, const float* sums, uint64_t len);
+/* Sets the iteration counter (after uploading storage from another run). */
+int dcfr_set_iterations(dcfr_solver* s, uint32_t t);
+
+/* One traversal from the root for traverser p with the opponent's root
+ * weights (cfr::traverse, cfr.rs:259-262): mode DCFR_MODE_*; iteration t
+ * picks the DCFR discount (Discount::new, cfr.rs:86-106) in CFR mode.
+ * Writes the root value row (n_p floats) to out. */
+int dcfr_traverse(dcfr_solver* s, int32_t p, int32_t mode, uint32_t t, float* out);
+
+/* Number of kernel launches the library issued on this handle so far. */
+int dcfr_kernel_launches(const dcfr_solver* s, uint64_t* out);
+
+/* Device time of the last dcfr_iterate call, in milliseconds (CUDA events
+ * on the handle's stream around the launches), and the algorithmic bytes
+ * one DCFR iteration moves (20 B per storage cell plus one opponent-reach
+ * row read and one value row write per node and traversal). */
+int dcfr_last_iterate_ms(dcfr_solver* s, double* ms);
+int dcfr_iteration_bytes(const dcfr_solver* s, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCFR_H */

@@ -1,0 +1,334 @@
+// C ABI of libdcfr (include/dcfr.h) over the device engine.
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/dcfr.h"
+#include "engine.hpp"
+
+struct dcfr_solver {
+  std::unique_ptr<dcfr::Engine> e;
+};
+
+static thread_local std::string g_error;
+
+static int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+static int done(const dcfr::Status& s) {
+  if (s.ok()) {
+    g_error.clear();
+    return DCFR_OK;
+  }
+  return fail(s.code, s.msg);
+}
+
+#define GUARD_BEGIN try {
+#define GUARD_END                                                     \
+  }                                                                   \
+  catch (const std::bad_alloc&) {                                     \
+    return fail(DCFR_ERR_OUT_OF_MEMORY, "host allocation failed");    \
+  }                                                                   \
+  catch (const std::exception& ex) {                                  \
+    return fail(DCFR_ERR_INVALID_ARG, ex.what());                     \
+  }
+
+static std::vector<dcfr_step> steps(const dcfr_step* path, size_t n) {
+  return path ? std::vector<dcfr_step>(path, path + n) : std::vector<dcfr_step>();
+}
+
+static void set_sizes(dcfr_street_sizes& s, std::initializer_list<double> bet_pot, double raise_mult) {
+  std::memset(&s, 0, sizeof s);
+  for (double b : bet_pot) s.bet[s.n_bet++] = dcfr_bet_size{DCFR_SIZE_POT, 0, b};
+  s.raise[s.n_raise++] = dcfr_bet_size{DCFR_SIZE_MULT, 0, raise_mult};
+}
+
+extern "C" {
+
+const char* dcfr_last_error(void) { return g_error.c_str(); }
+
+int dcfr_config_init(dcfr_config* cfg) {
+  if (!cfg) return fail(DCFR_ERR_INVALID_ARG, "cfg is NULL");
+  std::memset(cfg, 0, sizeof *cfg);
+  set_sizes(cfg->menu.flop, {0.33, 0.75}, 3.0);
+  set_sizes(cfg->menu.turn, {0.5, 1.0}, 3.0);
+  set_sizes(cfg->menu.river, {0.5, 1.0}, 3.0);
+  cfg->menu.max_raises = 3;
+  cfg->menu.add_allin_threshold = 1.5;
+  cfg->menu.force_allin_threshold = 0.15;
+  cfg->menu.merge_threshold = 0.1;
+  cfg->big_blind = 100;
+  cfg->max_memory_bytes = 8ull << 30;
+  cfg->storage = DCFR_STORAGE_AUTO;
+  cfg->isomorphism = 1;
+  cfg->dcfr.alpha = 1.5;
+  cfg->dcfr.beta = 0.0;
+  cfg->dcfr.gamma = 3.0;
+  cfg->dcfr.restart_average = 1;
+  cfg->dcfr.unweighted_average = 1;
+  return DCFR_OK;
+}
+
+int dcfr_estimate(const dcfr_config* cfg, dcfr_tree_stats* out) {
+  if (!cfg || !out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  dcfr::Game g;
+  std::string msg;
+  int rc = dcfr::build_game(*cfg, g, msg, false);
+  if (rc) return fail(rc, msg);
+  out->player_nodes = g.stats.player;
+  out->chance_nodes = g.stats.chance;
+  out->terminal_nodes = g.stats.terminal;
+  out->storage_cells = g.stats.cells;
+  out->compressed = g.compressed ? 1 : 0;
+  out->memory_bytes = dcfr::reference_memory_bytes(g.stats, g.compressed);
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_create(const dcfr_config* cfg, dcfr_solver** out) {
+  if (!cfg || !out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  GUARD_BEGIN
+  std::unique_ptr<dcfr::Engine> e;
+  dcfr::Status s = dcfr::Engine::create(*cfg, e);
+  if (!s.ok()) return done(s);
+  dcfr_solver* h = new dcfr_solver();
+  h->e = std::move(e);
+  *out = h;
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+void dcfr_destroy(dcfr_solver* s) { delete s; }
+
+#define NEED(h)                                                       \
+  if (!(h) || !(h)->e) return fail(DCFR_ERR_INVALID_ARG, "NULL solver")
+
+int dcfr_solve(dcfr_solver* s, const dcfr_solve_options* opts, const volatile int32_t* cancel, dcfr_progress_cb cb,
+               void* user, dcfr_progress* out) {
+  NEED(s);
+  if (!opts || !out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  return done(s->e->solve(*opts, cancel, cb, user, *out));
+  GUARD_END
+}
+
+int dcfr_iterate(dcfr_solver* s, uint32_t n) {
+  NEED(s);
+  GUARD_BEGIN
+  return done(s->e->iterate(n));
+  GUARD_END
+}
+
+int dcfr_synchronize(dcfr_solver* s) {
+  NEED(s);
+  return done(s->e->sync());
+}
+
+int dcfr_exploitability(dcfr_solver* s, double* out) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  return done(s->e->exploitability(*out));
+  GUARD_END
+}
+
+int dcfr_root_values(dcfr_solver* s, double out[2]) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  return done(s->e->root_values(out));
+  GUARD_END
+}
+
+int dcfr_iterations(const dcfr_solver* s, uint32_t* out) {
+  NEED(s);
+  *out = s->e->iterations;
+  return DCFR_OK;
+}
+
+int dcfr_last_exploitability(const dcfr_solver* s, double* out) {
+  NEED(s);
+  *out = s->e->last_exploitability;
+  return DCFR_OK;
+}
+
+int dcfr_stats(const dcfr_solver* s, dcfr_tree_stats* out) {
+  NEED(s);
+  const dcfr::Game& g = s->e->g;
+  out->player_nodes = g.stats.player;
+  out->chance_nodes = g.stats.chance;
+  out->terminal_nodes = g.stats.terminal;
+  out->storage_cells = g.stats.cells;
+  out->compressed = g.compressed ? 1 : 0;
+  out->memory_bytes = dcfr::reference_memory_bytes(g.stats, g.compressed);
+  return DCFR_OK;
+}
+
+int dcfr_isomorphic_pairs(const dcfr_solver* s, int32_t* out) {
+  NEED(s);
+  *out = s->e->isomorphic_pairs();
+  return DCFR_OK;
+}
+
+int dcfr_hands(const dcfr_solver* s, int32_t p, uint16_t* combos, float* weights, int32_t* n) {
+  NEED(s);
+  if (p < 0 || p > 1 || !n) return fail(DCFR_ERR_INVALID_ARG, "bad player");
+  const dcfr::Game& g = s->e->g;
+  *n = g.n[p];
+  if (combos) std::memcpy(combos, g.combos[p].data(), g.n[p] * 2);
+  if (weights) std::memcpy(weights, g.weights[p].data(), g.n[p] * 4);
+  return DCFR_OK;
+}
+
+int dcfr_is_decision(dcfr_solver* s, const dcfr_step* path, size_t n, int32_t* out) {
+  NEED(s);
+  GUARD_BEGIN
+  std::vector<dcfr::Act> acts;
+  bool dec = false;
+  dcfr::Status st = s->e->actions_at(steps(path, n), acts, dec);
+  *out = st.ok() && dec ? 1 : 0;
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_actions_at(dcfr_solver* s, const dcfr_step* path, size_t n, dcfr_action* actions, size_t cap,
+                    size_t* count) {
+  NEED(s);
+  GUARD_BEGIN
+  std::vector<dcfr::Act> acts;
+  bool dec = false;
+  dcfr::Status st = s->e->actions_at(steps(path, n), acts, dec);
+  if (!st.ok()) return done(st);
+  if (count) *count = acts.size();
+  for (size_t i = 0; i < acts.size() && i < cap && actions; i++) actions[i] = dcfr_action{acts[i].kind, 0, acts[i].amount};
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_query_sizes(dcfr_solver* s, const dcfr_step* path, size_t n, int32_t* num_actions, int32_t* num_hands) {
+  NEED(s);
+  GUARD_BEGIN
+  std::vector<dcfr::Act> acts;
+  bool dec = false;
+  dcfr::Status st = s->e->actions_at(steps(path, n), acts, dec);
+  if (!st.ok()) return done(st);
+  if (!dec) return fail(DCFR_ERR_BAD_PATH, "bad path: not a decision node");
+  // The acting player of the node reached by the path.
+  uint32_t node = 0;
+  {
+    // Re-walk cheaply through actions_at's node: the decision's player is
+    // read from the tree by following the same steps.
+    const dcfr::Game& g = s->e->g;
+    for (size_t i = 0; i < n; i++) {
+      const dcfr::GNode& nd = g.nodes[node];
+      if (nd.kind == dcfr::N_PLAYER) {
+        auto a = g.actions(node);
+        dcfr::Act want{path[i].action_kind, path[i].action_kind == DCFR_RAISE ? path[i].amount : 0};
+        node = nd.first + (uint32_t)(std::find(a.begin(), a.end(), want) - a.begin());
+      } else {
+        // Chance: any child has the same acting player at its root.
+        node = nd.first;
+      }
+    }
+  }
+  int q = s->e->g.nodes[node].player;
+  if (num_actions) *num_actions = (int32_t)acts.size();
+  if (num_hands) *num_hands = s->e->g.n[q];
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_query(dcfr_solver* s, const dcfr_step* path, size_t n, dcfr_node_info* info, dcfr_action* actions,
+               uint16_t* combos, float* strategy, float* ev, float* reach) {
+  NEED(s);
+  if (!info) return fail(DCFR_ERR_INVALID_ARG, "NULL info");
+  GUARD_BEGIN
+  std::vector<dcfr::Act> acts;
+  std::vector<uint16_t> cb;
+  std::vector<float> st, e, r;
+  dcfr::Status ss = s->e->query(steps(path, n), *info, acts, cb, st, e, r);
+  if (!ss.ok()) return done(ss);
+  if (actions)
+    for (size_t i = 0; i < acts.size(); i++) actions[i] = dcfr_action{acts[i].kind, 0, acts[i].amount};
+  if (combos) std::memcpy(combos, cb.data(), cb.size() * 2);
+  if (strategy) std::memcpy(strategy, st.data(), st.size() * 4);
+  if (ev) std::memcpy(ev, e.data(), e.size() * 4);
+  if (reach) std::memcpy(reach, r.data(), r.size() * 4);
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_ranges_after(dcfr_solver* s, const dcfr_step* path, size_t n, float out[2][DCFR_NUM_COMBOS]) {
+  NEED(s);
+  GUARD_BEGIN
+  return done(s->e->ranges_after(steps(path, n), out));
+  GUARD_END
+}
+
+int dcfr_storage_len(const dcfr_solver* s, uint64_t* len) {
+  NEED(s);
+  *len = s->e->g.storage_len;
+  return DCFR_OK;
+}
+
+int dcfr_download_storage(dcfr_solver* s, float* regrets, float* sums, uint64_t len) {
+  NEED(s);
+  if (len != s->e->g.storage_len) return fail(DCFR_ERR_INVALID_ARG, "storage length mismatch");
+  GUARD_BEGIN
+  return done(s->e->download(regrets, sums));
+  GUARD_END
+}
+
+int dcfr_upload_storage(dcfr_solver* s, const float* regrets, const float* sums, uint64_t len) {
+  NEED(s);
+  if (len != s->e->g.storage_len || !regrets || !sums) return fail(DCFR_ERR_INVALID_ARG, "storage length mismatch");
+  GUARD_BEGIN
+  return done(s->e->upload(regrets, sums));
+  GUARD_END
+}
+
+int dcfr_set_iterations(dcfr_solver* s, uint32_t t) {
+  NEED(s);
+  return done(s->e->set_iterations(t));
+}
+
+int dcfr_traverse(dcfr_solver* s, int32_t p, int32_t mode, uint32_t t, float* out) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL out");
+  GUARD_BEGIN
+  return done(s->e->traverse(p, mode, t, out));
+  GUARD_END
+}
+
+int dcfr_kernel_launches(const dcfr_solver* s, uint64_t* out) {
+  NEED(s);
+  *out = s->e->launches;
+  return DCFR_OK;
+}
+
+int dcfr_last_iterate_ms(dcfr_solver* s, double* ms) {
+  NEED(s);
+  *ms = s->e->last_iterate_ms;
+  return DCFR_OK;
+}
+
+int dcfr_iteration_bytes(const dcfr_solver* s, double* bytes) {
+  NEED(s);
+  *bytes = s->e->iteration_bytes();
+  return DCFR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,953 @@
+// Device engine of libdcfr (see engine.hpp): planning, device memory, graph
+// capture, the solve loop (Solver::run_solve, crates/solver/src/lib.rs:594-642),
+// exploitability (cfr.rs:482-502) and queries (lib.rs:735-912).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <unordered_map>
+
+namespace dcfr {
+
+Status cuda_status(cudaError_t e, const char* what) {
+  Status s;
+  if (e == cudaSuccess) return s;
+  s.code = (e == cudaErrorMemoryAllocation) ? DCFR_ERR_OUT_OF_MEMORY : DCFR_ERR_CUDA;
+  s.msg = std::string(what) + ": " + cudaGetErrorString(e);
+  return s;
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    Status _s = cuda_status((call), #call);       \
+    if (!_s.ok()) return _s;                      \
+  } while (0)
+
+template <class T>
+static Status dalloc(T*& p, size_t count, const char* what) {
+  p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    Status s = cuda_status(e, what);
+    s.msg += " (" + std::to_string(count * sizeof(T)) + " bytes)";
+    return s;
+  }
+  return Status();
+}
+
+template <class T>
+static void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+static inline int pad8(int n) { return (n + 7) & ~7; }
+
+Plan::~Plan() {
+  dfree(d_down);
+  dfree(d_up);
+  dfree(d_groups);
+  dfree(d_lanes);
+}
+
+// DcfrParams -> Discount (cfr.rs:86-106), host f64 pow as the reference.
+static DiscountD discount_for(uint32_t t, const dcfr_params& prm) {
+  uint32_t tm = t < 1 ? 1 : t;
+  double prev = (double)(tm - 1);
+  double pa = std::pow(prev, prm.alpha);
+  float neg = 0.0f;
+  if (!prm.beta_clip) {
+    double pb = std::pow(prev, prm.beta);
+    neg = (float)(pb / (pb + 1.0));
+  }
+  double since = (double)tm - 1.0;
+  if (prm.restart_average) {
+    uint32_t t0 = tm - 1;
+    uint32_t p4 = t0 == 0 ? 0 : (1u << ((31u - (uint32_t)__builtin_clz(t0)) & ~1u));
+    since = (double)(t0 - p4);
+  }
+  DiscountD d;
+  d.pos = (float)(pa / (pa + 1.0));
+  d.neg = neg;
+  d.strat = (float)std::pow(since / (since + 1.0), prm.gamma);
+  d.reach_weighted = prm.unweighted_average ? 0 : 1;
+  return d;
+}
+
+// next_check_gap (lib.rs:158-172).
+static uint32_t next_gap(bool has_prev, uint32_t t0, double e0, uint32_t t, double e, double target,
+                         uint32_t max_gap) {
+  uint32_t min_gap = std::max(max_gap / 4, 1u);
+  if (!has_prev) return max_gap;
+  if (!(e < e0 && e > target && t > t0 && target > 0.0)) return max_gap;
+  double k = std::log(e0 / e) / std::log((double)t / (double)t0);
+  double predicted = (double)t * std::pow(e / target, 1.0 / k);
+  double gap = std::ceil(predicted - (double)t);
+  if (!std::isfinite(gap)) return max_gap;
+  double gg = gap > 0.0 ? gap : 0.0;
+  uint32_t gu = gg >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)gg;
+  return std::min(std::max(gu, min_gap), max_gap);
+}
+
+Status Engine::create(const dcfr_config& cfg, std::unique_ptr<Engine>& out) {
+  std::unique_ptr<Engine> e(new Engine());
+  Status s;
+  s.code = build_game(cfg, e->g, s.msg, true);
+  if (!s.ok()) return s;
+  s = e->init();
+  if (!s.ok()) return s;
+  out = std::move(e);
+  return Status();
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  free_graphs();
+  full_[0].reset();
+  full_[1].reset();
+  dfree(regrets_);
+  dfree(sums_);
+  dfree(reach_);
+  dfree(vals_);
+  dfree(alive_);
+  dfree(root_rows_);
+  dfree(root_out_);
+  for (int q = 0; q < 2; q++) {
+    dfree(hc1_[q]);
+    dfree(hc2_[q]);
+    dfree(same_[q]);
+  }
+  dfree(perm_);
+  dfree(chance_cards_);
+  dfree(iso_);
+  dfree(tables_);
+  dfree(table_count_);
+  dfree(scratch_);
+  dfree(disc_table_);
+  dfree(cur_disc_);
+  dfree(counter_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::free_graphs() {
+  if (iter_graph_) cudaGraphExecDestroy(iter_graph_);
+  if (br_graph_) cudaGraphExecDestroy(br_graph_);
+  if (avg_graph_) cudaGraphExecDestroy(avg_graph_);
+  iter_graph_ = br_graph_ = avg_graph_ = nullptr;
+}
+
+int Engine::isomorphic_pairs() const {
+  int k = 0;
+  for (int i = 0; i < 6; i++) k += g.sym[i];
+  return k;
+}
+
+// Algorithmic bytes of one DCFR iteration: every decision node is once the
+// traverser's (regret read + write) and once the opponent's (regret read,
+// strategy-sum read + write): 20 B per storage cell; plus, per traversal,
+// one opponent-reach row read and one value row write per node.
+double Engine::iteration_bytes() const {
+  double cells = (double)g.storage_len;
+  double nodes = (double)g.nodes.size();
+  return 20.0 * cells + 2.0 * nodes * 4.0 * ((double)g.n[0] + (double)g.n[1]);
+}
+
+Status Engine::init() {
+  last_exploitability = INFINITY;
+  CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&ev0_));
+  CK(cudaEventCreate(&ev1_));
+  CK(terminal_kernel_setup());
+  hp_[0] = pad8(g.n[0]);
+  hp_[1] = pad8(g.n[1]);
+  stride_ = std::max(hp_[0], hp_[1]);
+  const size_t N = g.nodes.size();
+
+  // Storage layout: one [actions][hp_q] block per decision node, in the
+  // reference's node order (Node::offset, tree.rs:462, 468).
+  std::vector<uint32_t> players;
+  for (uint32_t v = 0; v < N; v++)
+    if (g.nodes[v].kind == N_PLAYER) players.push_back(v);
+  std::sort(players.begin(), players.end(),
+            [&](uint32_t a, uint32_t b) { return g.nodes[a].ref_offset < g.nodes[b].ref_offset; });
+  gpu_off_.assign(N, 0);
+  gpu_len_ = 0;
+  for (uint32_t v : players) {
+    gpu_off_[v] = gpu_len_;
+    gpu_len_ += (uint64_t)g.nodes[v].nchild * (uint64_t)hp_[g.nodes[v].player];
+  }
+  Status s;
+  if (!(s = dalloc(regrets_, gpu_len_, "storage")).ok()) return s;
+  if (!(s = dalloc(sums_, gpu_len_, "storage")).ok()) return s;
+  CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
+  CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
+
+  // Hands.
+  for (int q = 0; q < 2; q++) {
+    std::vector<uint8_t> a(hp_[q], 255), b(hp_[q], 255);
+    std::vector<uint32_t> sm(hp_[q], NO);
+    for (int i = 0; i < g.n[q]; i++) {
+      a[i] = g.c1[q][i];
+      b[i] = g.c2[q][i];
+      sm[i] = g.same[q][i];
+    }
+    if (!(s = dalloc(hc1_[q], hp_[q], "hands")).ok()) return s;
+    if (!(s = dalloc(hc2_[q], hp_[q], "hands")).ok()) return s;
+    if (!(s = dalloc(same_[q], hp_[q], "hands")).ok()) return s;
+    CK(cudaMemcpy(hc1_[q], a.data(), hp_[q], cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(hc2_[q], b.data(), hp_[q], cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(same_[q], sm.data(), hp_[q] * 4, cudaMemcpyHostToDevice));
+  }
+  {
+    std::vector<uint16_t> perm((size_t)12 * stride_, 0);
+    for (int q = 0; q < 2; q++)
+      for (int pr = 0; pr < 6; pr++)
+        for (size_t h = 0; h < g.perm[q][pr].size(); h++) perm[(size_t)(q * 6 + pr) * stride_ + h] = g.perm[q][pr][h];
+    if (!(s = dalloc(perm_, perm.size(), "perm")).ok()) return s;
+    CK(cudaMemcpy(perm_, perm.data(), perm.size() * 2, cudaMemcpyHostToDevice));
+  }
+  // Chance cards and isomorphic references.
+  {
+    std::vector<uint8_t> cc;
+    std::vector<IsoRefD> iso;
+    cc_off_.assign(g.chance.size(), 0);
+    iso_first_.assign(g.chance.size(), 0);
+    for (uint32_t v = 0; v < N; v++) {
+      const GNode& nd = g.nodes[v];
+      if (nd.kind != N_CHANCE) continue;
+      cc_off_[nd.index] = (uint32_t)cc.size();
+      for (uint32_t c = nd.first; c < nd.first + nd.nchild; c++) cc.push_back((uint8_t)g.nodes[c].card);
+      iso_first_[nd.index] = (uint32_t)iso.size();
+      const ChanceIso& ci = g.chance[nd.index];
+      for (size_t r = 0; r < ci.ci.size(); r++) iso.push_back(IsoRefD{ci.ci[r], ci.pair[r], 0});
+    }
+    if (!(s = dalloc(chance_cards_, cc.size(), "chance cards")).ok()) return s;
+    if (!cc.empty()) CK(cudaMemcpy(chance_cards_, cc.data(), cc.size(), cudaMemcpyHostToDevice));
+    if (!(s = dalloc(iso_, iso.size(), "iso refs")).ok()) return s;
+    if (!iso.empty()) CK(cudaMemcpy(iso_, iso.data(), iso.size() * sizeof(IsoRefD), cudaMemcpyHostToDevice));
+  }
+  // Strength tables, built on the device.
+  {
+    const int nb = (int)g.boards.size();
+    tstride_ = std::max(g.n[0], g.n[1]);
+    if (!(s = dalloc(tables_, (size_t)std::max(nb, 1) * 2 * tstride_, "strength tables")).ok()) return s;
+    if (!(s = dalloc(table_count_, (size_t)std::max(nb, 1) * 2, "strength tables")).ok()) return s;
+    if (nb > 0) {
+      std::vector<uint8_t> bc((size_t)nb * 5);
+      for (int b = 0; b < nb; b++)
+        for (int k = 0; k < 5; k++) bc[(size_t)b * 5 + k] = (uint8_t)g.boards[b][k];
+      uint8_t* d_boards = nullptr;
+      if (!(s = dalloc(d_boards, bc.size(), "boards")).ok()) return s;
+      CK(cudaMemcpy(d_boards, bc.data(), bc.size(), cudaMemcpyHostToDevice));
+      launch_strength(d_boards, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1], tables_, table_count_,
+                      tstride_, stream_);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(stream_));
+      cudaFree(d_boards);
+    }
+  }
+  // Plans for the two traversals of an iteration.
+  for (int p = 0; p < 2; p++) {
+    full_[p].reset(new Plan());
+    if (!(s = build_plan(0, p, *full_[p])).ok()) return s;
+    max_slots_ = std::max<uint64_t>(max_slots_, full_[p]->nslots);
+  }
+  // Rows.
+  if (!(s = dalloc(reach_, (size_t)max_slots_ * stride_, "reach rows")).ok()) return s;
+  if (!(s = dalloc(vals_, (size_t)N * stride_, "value rows")).ok()) return s;
+  if (!(s = dalloc(alive_, (size_t)max_slots_, "liveness flags")).ok()) return s;
+  CK(cudaMemsetAsync(reach_, 0, (size_t)max_slots_ * stride_ * 4, stream_));
+  CK(cudaMemsetAsync(vals_, 0, (size_t)N * stride_ * 4, stream_));
+  {
+    std::vector<float> rr((size_t)2 * stride_, 0.0f);
+    for (int p = 0; p < 2; p++)
+      for (int i = 0; i < g.n[p ^ 1]; i++) rr[(size_t)p * stride_ + i] = g.weights[p ^ 1][i];
+    if (!(s = dalloc(root_rows_, rr.size(), "root rows")).ok()) return s;
+    CK(cudaMemcpy(root_rows_, rr.data(), rr.size() * 4, cudaMemcpyHostToDevice));
+    if (!(s = dalloc(root_out_, rr.size(), "root rows")).ok()) return s;
+  }
+  // Terminal scratch: one [nmax][32] f64 block per resident warp.
+  {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    term_blocks_ = sms * 2;
+    if (!(s = dalloc(scratch_, (size_t)term_blocks_ * TERM_WARPS * tstride_ * 32, "terminal scratch")).ok())
+      return s;
+  }
+  for (int p = 0; p < 2; p++)
+    if (!(s = upload_plan(*full_[p])).ok()) return s;
+  if (!(s = dalloc(cur_disc_, 1, "discounts")).ok()) return s;
+  if (!(s = dalloc(counter_, 1, "counter")).ok()) return s;
+  CK(cudaMemsetAsync(counter_, 0, 4, stream_));
+  if (!(s = ensure_discounts(1024)).ok()) return s;
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// Level-synchronous plan of one traversal (see plan.hpp).
+Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
+  plan.p = p;
+  plan.root = root;
+  const int o = p ^ 1;
+  std::vector<std::vector<DownTask>> down;
+  std::vector<std::vector<UpTask>> up;
+  std::vector<int> dmax, umax;
+  struct SdLane {
+    uint32_t kind, board;
+    TermLane lane;
+  };
+  std::vector<SdLane> sd;
+  std::vector<TermLane> folds[2];
+  uint32_t next_slot = 1;
+  std::deque<std::pair<uint32_t, uint32_t>> q;  // node, depth
+  std::vector<uint32_t> slot_of;                // by BFS discovery, indexed via map below
+  std::vector<uint32_t> node_slot;
+  // Slots of nodes in the subtree (node ids may be sparse for subtrees).
+  std::unordered_map<uint32_t, uint32_t> slot;
+  slot[root] = 0;
+  q.push_back({root, 0});
+  const double hp = g.half_pot, norm = g.norm;
+  uint64_t count = 0;
+  while (!q.empty()) {
+    auto [v, depth] = q.front();
+    q.pop_front();
+    count++;
+    const GNode& nd = g.nodes[v];
+    const uint32_t sv = slot[v];
+    if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
+      if (down.size() <= depth) {
+        down.resize(depth + 1);
+        up.resize(depth + 1);
+        dmax.resize(depth + 1, 0);
+        umax.resize(depth + 1, 0);
+      }
+      if (nd.nchild > MAX_ACTIONS && nd.kind == N_PLAYER) {
+        Status s;
+        s.code = DCFR_ERR_INVALID_ARG;
+        s.msg = "a decision node has more than 16 actions";
+        return s;
+      }
+      bool own = nd.kind == N_PLAYER && nd.player == p;
+      uint32_t first_slot = own ? sv : next_slot;
+      if (!own) next_slot += nd.nchild;
+      for (uint32_t i = 0; i < nd.nchild; i++) {
+        uint32_t c = nd.first + i;
+        slot[c] = own ? sv : first_slot + i;
+        q.push_back({c, depth + 1});
+      }
+      if (nd.kind == N_PLAYER) {
+        if (!own) {
+          DownTask t{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f};
+          down[depth].push_back(t);
+          dmax[depth] = std::max<int>(dmax[depth], nd.nchild);
+        }
+        UpTask u{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild, first_slot, gpu_off_[v],
+                 0, 0, 0, 0};
+        up[depth].push_back(u);
+        umax[depth] = std::max<int>(umax[depth], nd.nchild);
+      } else {
+        DownTask t{D_CHANCE_SPLIT, sv, first_slot, nd.nchild, 0, cc_off_[nd.index], nd.factor};
+        down[depth].push_back(t);
+        UpTask u{U_CHANCE_SUM, sv, v, nd.first, nd.nchild, first_slot, 0, cc_off_[nd.index], iso_first_[nd.index],
+                 (uint32_t)g.chance[nd.index].ci.size(), 0};
+        up[depth].push_back(u);
+      }
+    } else {
+      // Terminal. Batched evaluation (river.rs) iff the terminal sits below a
+      // river decision node inside this traversal (cfr.rs:282-284).
+      bool batch = v != root && nd.parent != NO && g.nodes[nd.parent].kind == N_PLAYER &&
+                   g.nodes[nd.parent].street == DCFR_RIVER;
+      TermLane L{sv, v, NONE32, 0, 0.0, 0.0, 0.0, 0.0};
+      if (nd.kind == N_FOLD) {
+        // fold_payoff (cfr.rs:226-235).
+        int f = nd.player;
+        double val = f == p ? -(hp + (double)nd.invest[p]) : hp + (double)nd.invest[f] - (double)nd.rake;
+        L.a = val * norm;
+        if (batch) {
+          // A fold next to a showdown under the traverser's own decision
+          // shares its reach and is read off the showdown sweep
+          // (river.rs:190-240).
+          const GNode& par = g.nodes[nd.parent];
+          bool paired = false;
+          if (par.player == p)
+            for (uint32_t c = par.first; c < par.first + par.nchild; c++)
+              if (g.nodes[c].kind == N_SHOWDOWN) paired = true;
+          if (paired) continue;
+        }
+        folds[batch ? 1 : 0].push_back(L);
+      } else {
+        // showdown_payoffs (cfr.rs:239-246).
+        double rake = (double)nd.rake;
+        L.a = (hp + (double)nd.invest[o] - rake) * norm;
+        L.b = -(hp + (double)nd.invest[p]) * norm;
+        L.c = 0.5 * ((double)(nd.invest[o] - nd.invest[p]) - rake) * norm;
+        if (batch) {
+          const GNode& par = g.nodes[nd.parent];
+          if (par.player == p)
+            for (uint32_t c = par.first; c < par.first + par.nchild; c++)
+              if (g.nodes[c].kind == N_FOLD) {
+                const GNode& fn = g.nodes[c];
+                int f = fn.player;
+                double val = f == p ? -(hp + (double)fn.invest[p]) : hp + (double)fn.invest[f] - (double)fn.rake;
+                L.frow = c;
+                L.d = val * norm;
+              }
+        }
+        sd.push_back(SdLane{batch ? (uint32_t)T_SHOWDOWN_BATCH : (uint32_t)T_SHOWDOWN_SCALAR, nd.index, L});
+      }
+    }
+  }
+  plan.nodes = count;
+  plan.nslots = next_slot;
+  // Flatten levels.
+  plan.h_down.clear();
+  plan.h_up.clear();
+  plan.down.assign(down.size(), Plan::Level());
+  plan.up.assign(up.size(), Plan::Level());
+  for (size_t d = 0; d < down.size(); d++) {
+    plan.down[d] = Plan::Level{(uint32_t)plan.h_down.size(), (uint32_t)down[d].size(), dmax[d]};
+    plan.h_down.insert(plan.h_down.end(), down[d].begin(), down[d].end());
+    plan.up[d] = Plan::Level{(uint32_t)plan.h_up.size(), (uint32_t)up[d].size(), umax[d]};
+    plan.h_up.insert(plan.h_up.end(), up[d].begin(), up[d].end());
+  }
+  // Terminal groups: showdowns by (kind, board), folds by kind, 32 lanes each.
+  std::stable_sort(sd.begin(), sd.end(), [](const SdLane& a, const SdLane& b) {
+    return a.kind != b.kind ? a.kind < b.kind : a.board < b.board;
+  });
+  plan.h_groups.clear();
+  plan.h_lanes.clear();
+  for (size_t i = 0; i < sd.size();) {
+    size_t j = i;
+    while (j < sd.size() && j - i < 32 && sd[j].kind == sd[i].kind && sd[j].board == sd[i].board) j++;
+    TermGroup G{sd[i].kind, sd[i].board, (uint32_t)plan.h_lanes.size(), (uint32_t)(j - i)};
+    for (size_t k = i; k < j; k++) plan.h_lanes.push_back(sd[k].lane);
+    plan.h_groups.push_back(G);
+    i = j;
+  }
+  for (int b = 0; b < 2; b++)
+    for (size_t i = 0; i < folds[b].size(); i += 32) {
+      size_t j = std::min(folds[b].size(), i + 32);
+      TermGroup G{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, 0, (uint32_t)plan.h_lanes.size(),
+                  (uint32_t)(j - i)};
+      for (size_t k = i; k < j; k++) plan.h_lanes.push_back(folds[b][k]);
+      plan.h_groups.push_back(G);
+    }
+  int kernels = 0;
+  for (auto& l : plan.down) kernels += l.count > 0;
+  for (auto& l : plan.up) kernels += l.count > 0;
+  kernels += plan.h_groups.empty() ? 0 : 1;
+  plan.kernels = kernels;
+  return Status();
+}
+
+Status Engine::upload_plan(Plan& plan) {
+  Status s;
+  if (!(s = dalloc(plan.d_down, plan.h_down.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_up, plan.h_up.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_groups, plan.h_groups.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_lanes, plan.h_lanes.size(), "plan")).ok()) return s;
+  if (!plan.h_down.empty())
+    CK(cudaMemcpy(plan.d_down, plan.h_down.data(), plan.h_down.size() * sizeof(DownTask), cudaMemcpyHostToDevice));
+  if (!plan.h_up.empty())
+    CK(cudaMemcpy(plan.d_up, plan.h_up.data(), plan.h_up.size() * sizeof(UpTask), cudaMemcpyHostToDevice));
+  if (!plan.h_groups.empty())
+    CK(cudaMemcpy(plan.d_groups, plan.h_groups.data(), plan.h_groups.size() * sizeof(TermGroup),
+                  cudaMemcpyHostToDevice));
+  if (!plan.h_lanes.empty())
+    CK(cudaMemcpy(plan.d_lanes, plan.h_lanes.data(), plan.h_lanes.size() * sizeof(TermLane), cudaMemcpyHostToDevice));
+  return Status();
+}
+
+void Engine::row_args(int p, RowArgs& A) const {
+  A.regrets = regrets_;
+  A.sums = sums_;
+  A.reach = reach_;
+  A.vals = vals_;
+  A.alive = alive_;
+  for (int q = 0; q < 2; q++) {
+    A.hc1[q] = hc1_[q];
+    A.hc2[q] = hc2_[q];
+    A.n[q] = g.n[q];
+    A.hp[q] = hp_[q];
+  }
+  A.perm = perm_;
+  A.chance_cards = chance_cards_;
+  A.iso = iso_;
+  A.disc = cur_disc_;
+  A.stride = stride_;
+  A.p = p;
+}
+
+void Engine::term_args(int p, TermArgs& A) const {
+  A.reach = reach_;
+  A.vals = vals_;
+  A.alive = alive_;
+  A.scratch = scratch_;
+  A.tables = tables_;
+  A.table_count = table_count_;
+  for (int q = 0; q < 2; q++) {
+    A.hc1[q] = hc1_[q];
+    A.hc2[q] = hc2_[q];
+    A.same[q] = same_[q];
+    A.n[q] = g.n[q];
+    A.hp[q] = hp_[q];
+  }
+  A.stride = stride_;
+  A.tstride = tstride_;
+  A.nmax = tstride_;
+  A.p = p;
+}
+
+// Enqueues one traversal: liveness reset, root row, down levels, terminals,
+// up levels (deepest first); the root's value row is copied to root_out.
+void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out) {
+  const int p = plan.p, o = p ^ 1;
+  cudaMemsetAsync(alive_, 0, (size_t)plan.nslots * 4, stream_);
+  cudaMemsetAsync(alive_, 1, 4, stream_);
+  cudaMemcpyAsync(reach_, root_row, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice, stream_);
+  RowArgs A;
+  row_args(p, A);
+  const int dchunks = (hp_[o] + ROW_CHUNK - 1) / ROW_CHUNK;
+  const int uchunks = (hp_[p] + ROW_CHUNK - 1) / ROW_CHUNK;
+  for (const Plan::Level& l : plan.down)
+    if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, dchunks, stream_);
+  if (!plan.h_groups.empty()) {
+    TermArgs T;
+    term_args(p, T);
+    int ng = (int)plan.h_groups.size();
+    int blocks = std::min(term_blocks_, (ng + TERM_WARPS - 1) / TERM_WARPS);
+    launch_terminal(T, plan.d_groups, plan.d_lanes, ng, blocks, stream_);
+  }
+  for (size_t d = plan.up.size(); d-- > 0;) {
+    const Plan::Level& l = plan.up[d];
+    if (l.count) launch_up(mode, l.maxa, A, plan.d_up + l.first, (int)l.count, uchunks, stream_);
+  }
+  if (root_out)
+    cudaMemcpyAsync(root_out, vals_ + (size_t)plan.root * stride_, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice,
+                    stream_);
+}
+
+Status Engine::ensure_discounts(uint32_t max_t) {
+  if (disc_table_ && max_t < disc_len_) return Status();
+  uint32_t len = std::max<uint32_t>(max_t + 1, disc_len_ * 2);
+  std::vector<DiscountD> tab(len);
+  for (uint32_t t = 0; t < len; t++) tab[t] = discount_for(t, g.cfg.dcfr);
+  CK(cudaStreamSynchronize(stream_));
+  free_graphs();
+  dfree(disc_table_);
+  Status s;
+  if (!(s = dalloc(disc_table_, len, "discounts")).ok()) return s;
+  CK(cudaMemcpy(disc_table_, tab.data(), len * sizeof(DiscountD), cudaMemcpyHostToDevice));
+  disc_len_ = len;
+  return Status();
+}
+
+Status Engine::capture_graphs() {
+  if (iter_graph_) return Status();
+  cudaGraph_t graph;
+  // One DCFR iteration: t += 1, then player 0's and player 1's traversals
+  // with the same discounts (lib.rs:577-585).
+  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  launch_advance(counter_, disc_table_, disc_len_, cur_disc_, stream_);
+  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr);
+  enqueue_traversal(*full_[1], M_CFR, root_rows_ + stride_, nullptr);
+  CK(cudaStreamEndCapture(stream_, &graph));
+  CK(cudaGraphInstantiate(&iter_graph_, graph, 0));
+  cudaGraphDestroy(graph);
+  iter_kernels_ = 1 + full_[0]->kernels + full_[1]->kernels;
+  for (int mode : {M_BR, M_AVG}) {
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    enqueue_traversal(*full_[0], mode, root_rows_, root_out_);
+    enqueue_traversal(*full_[1], mode, root_rows_ + stride_, root_out_ + stride_);
+    CK(cudaStreamEndCapture(stream_, &graph));
+    CK(cudaGraphInstantiate(mode == M_BR ? &br_graph_ : &avg_graph_, graph, 0));
+    cudaGraphDestroy(graph);
+  }
+  pair_kernels_ = full_[0]->kernels + full_[1]->kernels;
+  return Status();
+}
+
+Status Engine::iterate(uint32_t n) {
+  Status s;
+  if (!(s = ensure_discounts(iterations + n + 1)).ok()) return s;
+  if (!(s = capture_graphs()).ok()) return s;
+  CK(cudaEventRecord(ev0_, stream_));
+  for (uint32_t i = 0; i < n; i++) {
+    CK(cudaGraphLaunch(iter_graph_, stream_));
+    launches += iter_kernels_;
+  }
+  CK(cudaEventRecord(ev1_, stream_));
+  iterations += n;
+  CK(cudaEventSynchronize(ev1_));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_iterate_ms = ms;
+  return Status();
+}
+
+Status Engine::sync() {
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// root_values (cfr.rs:482-490): sum over hands of value * weight in f64.
+Status Engine::mode_root_values(int mode, double out[2]) {
+  Status s;
+  if (!(s = capture_graphs()).ok()) return s;
+  CK(cudaGraphLaunch(mode == M_BR ? br_graph_ : avg_graph_, stream_));
+  launches += pair_kernels_;
+  std::vector<float> rows((size_t)2 * stride_);
+  CK(cudaMemcpyAsync(rows.data(), root_out_, rows.size() * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  for (int p = 0; p < 2; p++) {
+    double acc = -0.0;
+    for (int h = 0; h < g.n[p]; h++) acc += (double)rows[(size_t)p * stride_ + h] * (double)g.weights[p][h];
+    out[p] = acc;
+  }
+  return Status();
+}
+
+// exploitability (cfr.rs:494-502).
+Status Engine::exploitability(double& out) {
+  double br[2];
+  Status s = mode_root_values(M_BR, br);
+  if (!s.ok()) return s;
+  if (g.cfg.rake_rate > 0.0 && g.cfg.rake_cap > 0.0) {
+    double ev[2];
+    if (!(s = mode_root_values(M_AVG, ev)).ok()) return s;
+    out = ((br[0] - ev[0]) + (br[1] - ev[1])) / 2.0;
+  } else {
+    out = (br[0] + br[1]) / 2.0;
+  }
+  return Status();
+}
+
+Status Engine::root_values(double out[2]) { return mode_root_values(M_AVG, out); }
+
+Status Engine::traverse(int p, int mode, uint32_t t, float* out) {
+  if (p < 0 || p > 1 || mode < 0 || mode > 2) {
+    Status s;
+    s.code = DCFR_ERR_INVALID_ARG;
+    s.msg = "traverse: bad player or mode";
+    return s;
+  }
+  DiscountD d = discount_for(t, g.cfg.dcfr);
+  CK(cudaMemcpyAsync(cur_disc_, &d, sizeof d, cudaMemcpyHostToDevice, stream_));
+  enqueue_traversal(*full_[p], mode, root_rows_ + (size_t)p * stride_, root_out_ + (size_t)p * stride_);
+  launches += full_[p]->kernels;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, root_out_ + (size_t)p * stride_, (size_t)g.n[p] * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+Status Engine::solve(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb, void* user,
+                     dcfr_progress& progress) {
+  const double pot = (double)g.cfg.root.pot;
+  const uint32_t check_every = std::max(opts.check_every, 1u);
+  progress.iteration = iterations;
+  progress.max_iterations = opts.max_iterations;
+  progress.exploitability = last_exploitability;
+  progress.exploitability_pct = 100.0 * last_exploitability / pot;
+  progress.finished = 0;
+  const double target = opts.target_exploitability_pct * pot / 100.0;
+  uint32_t next_check = iterations + check_every;
+  bool has_last = false;
+  uint32_t last_t = 0;
+  double last_e = 0.0;
+  Status s;
+  if (!(s = ensure_discounts(opts.max_iterations + 1)).ok()) return s;
+  if (!(s = capture_graphs()).ok()) return s;
+  while (iterations < opts.max_iterations) {
+    if (cancel && *cancel) {
+      progress.finished = 1;
+      CK(cudaStreamSynchronize(stream_));
+      return Status();
+    }
+    iterations += 1;
+    CK(cudaGraphLaunch(iter_graph_, stream_));
+    launches += iter_kernels_;
+    bool last = iterations >= opts.max_iterations;
+    if (iterations >= next_check || last) {
+      double e;
+      if (!(s = exploitability(e)).ok()) return s;
+      last_exploitability = e;
+      progress.iteration = iterations;
+      progress.exploitability = e;
+      progress.exploitability_pct = 100.0 * e / pot;
+      bool done = progress.exploitability_pct <= opts.target_exploitability_pct || last;
+      progress.finished = done ? 1 : 0;
+      bool keep = cb ? cb(&progress, user) != 0 : true;
+      if (done || !keep) {
+        progress.finished = 1;
+        return Status();
+      }
+      uint32_t t = iterations;
+      next_check = t + next_gap(has_last, last_t, last_e, t, e, target, check_every);
+      has_last = true;
+      last_t = t;
+      last_e = e;
+    }
+  }
+  progress.finished = 1;
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+Status Engine::download(float* regrets, float* sums) {
+  std::vector<float> r(gpu_len_), sm(gpu_len_);
+  CK(cudaMemcpyAsync(r.data(), regrets_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(sm.data(), sums_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  for (uint32_t v = 0; v < g.nodes.size(); v++) {
+    const GNode& nd = g.nodes[v];
+    if (nd.kind != N_PLAYER) continue;
+    int q = nd.player, n = g.n[q];
+    for (int a = 0; a < nd.nchild; a++) {
+      if (regrets)
+        std::memcpy(regrets + nd.ref_offset + (size_t)a * n, r.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 4);
+      if (sums) std::memcpy(sums + nd.ref_offset + (size_t)a * n, sm.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 4);
+    }
+  }
+  return Status();
+}
+
+Status Engine::upload(const float* regrets, const float* sums) {
+  std::vector<float> r(gpu_len_, 0.0f), sm(gpu_len_, 0.0f);
+  for (uint32_t v = 0; v < g.nodes.size(); v++) {
+    const GNode& nd = g.nodes[v];
+    if (nd.kind != N_PLAYER) continue;
+    int q = nd.player, n = g.n[q];
+    for (int a = 0; a < nd.nchild; a++) {
+      std::memcpy(r.data() + gpu_off_[v] + (size_t)a * hp_[q], regrets + nd.ref_offset + (size_t)a * n, n * 4);
+      std::memcpy(sm.data() + gpu_off_[v] + (size_t)a * hp_[q], sums + nd.ref_offset + (size_t)a * n, n * 4);
+    }
+  }
+  CK(cudaMemcpyAsync(regrets_, r.data(), gpu_len_ * 4, cudaMemcpyHostToDevice, stream_));
+  CK(cudaMemcpyAsync(sums_, sm.data(), gpu_len_ * 4, cudaMemcpyHostToDevice, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+Status Engine::set_iterations(uint32_t t) {
+  iterations = t;
+  CK(cudaMemcpyAsync(counter_, &iterations, 4, cudaMemcpyHostToDevice, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// Average strategy of a node (lib.rs:735-743) from the device sums.
+Status Engine::avg_strategy(uint32_t node, std::vector<float>& s) {
+  const GNode& nd = g.nodes[node];
+  int q = nd.player, n = g.n[q];
+  std::vector<float> blk((size_t)nd.nchild * hp_[q]);
+  CK(cudaMemcpyAsync(blk.data(), sums_ + gpu_off_[node], blk.size() * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  s.assign((size_t)nd.nchild * n, 0.0f);
+  for (int a = 0; a < nd.nchild; a++)
+    std::memcpy(s.data() + (size_t)a * n, blk.data() + (size_t)a * hp_[q], n * 4);
+  normalize_rows(s.data(), nd.nchild, n);
+  return Status();
+}
+
+static Status bad_path(const std::string& m) {
+  Status s;
+  s.code = DCFR_ERR_BAD_PATH;
+  s.msg = "bad path: " + m;
+  return s;
+}
+
+static const char* RANKC = "23456789TJQKA";
+static const char* SUITC = "cdhs";
+static std::string card_name(int c) { return std::string(1, RANKC[c >> 2]) + SUITC[c & 3]; }
+
+// walk (lib.rs:746-825).
+Status Engine::walk(const std::vector<dcfr_step>& path, uint32_t& node, std::vector<float> reach[2],
+                    std::vector<uint32_t> to_canon[2]) {
+  static const uint8_t PAIRS[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+  uint32_t id = 0;
+  for (int x = 0; x < 2; x++) {
+    reach[x] = g.weights[x];
+    to_canon[x].resize(g.n[x]);
+    for (int i = 0; i < g.n[x]; i++) to_canon[x][i] = (uint32_t)i;
+  }
+  int suit_map[4] = {0, 1, 2, 3};
+  for (size_t depth = 0; depth < path.size(); depth++) {
+    const dcfr_step& st = path[depth];
+    const GNode nd = g.nodes[id];
+    if (nd.kind == N_PLAYER && st.kind == 0) {
+      auto acts = g.actions(id);
+      Act a{st.action_kind, st.action_kind == DCFR_RAISE ? st.amount : 0};
+      size_t ai = std::find(acts.begin(), acts.end(), a) - acts.begin();
+      if (ai == acts.size()) return bad_path("action not available at depth " + std::to_string(depth));
+      int q = nd.player, n = g.n[q];
+      std::vector<float> s;
+      Status ss = avg_strategy(id, s);
+      if (!ss.ok()) return ss;
+      for (int i = 0; i < n; i++) reach[q][i] *= s[ai * n + i];
+      id = nd.first + (uint32_t)ai;
+    } else if (nd.kind == N_CHANCE && st.kind == 1) {
+      int c = st.card;
+      if (c < 0 || c >= 52) return bad_path("card id out of range at depth " + std::to_string(depth));
+      int cc = (c >> 2) * 4 + suit_map[c & 3];
+      int canonical = -1;
+      for (uint32_t ch = nd.first; ch < nd.first + nd.nchild; ch++)
+        if (g.nodes[ch].card == cc) {
+          id = ch;
+          canonical = cc;
+          break;
+        }
+      if (canonical < 0) {
+        const ChanceIso& info = g.chance[nd.index];
+        size_t j = std::find(info.cards.begin(), info.cards.end(), (uint8_t)cc) - info.cards.begin();
+        if (j == info.cards.size())
+          return bad_path("card " + card_name(c) + " not in the tree at depth " + std::to_string(depth));
+        int ci = info.ci[j], pair = info.pair[j];
+        int a = PAIRS[pair][0], b = PAIRS[pair][1];
+        for (int& sm : suit_map) sm = sm == a ? b : sm == b ? a : sm;
+        for (int x = 0; x < 2; x++) {
+          const auto& perm = g.perm[x][pair];
+          std::vector<float> r2(reach[x].size(), 0.0f);
+          for (size_t h = 0; h < reach[x].size(); h++) r2[perm[h]] = reach[x][h];
+          reach[x] = r2;
+          for (auto& t : to_canon[x]) t = perm[t];
+        }
+        id = nd.first + (uint32_t)ci;
+        canonical = g.nodes[id].card;
+      }
+      for (int x = 0; x < 2; x++)
+        for (uint32_t k : g.blocked[x][canonical]) reach[x][k] = 0.0f;
+    } else {
+      return bad_path("step doesn't match node kind at depth " + std::to_string(depth));
+    }
+  }
+  node = id;
+  return Status();
+}
+
+Status Engine::actions_at(const std::vector<dcfr_step>& path, std::vector<Act>& out, bool& decision) {
+  uint32_t node;
+  std::vector<float> reach[2];
+  std::vector<uint32_t> tc[2];
+  Status s = walk(path, node, reach, tc);
+  if (!s.ok()) return s;
+  decision = g.nodes[node].kind == N_PLAYER;
+  out.clear();
+  if (decision) out = g.actions(node);
+  return Status();
+}
+
+// Values of traverser p at the subtree `root` under the opponent reach
+// (cfr::traverse in Average mode from an interior node).
+Status Engine::subtree_values(uint32_t root, int p, const std::vector<float>& opp_reach, std::vector<float>& out) {
+  out.assign(g.n[p], 0.0f);
+  bool any = false;
+  for (float x : opp_reach) any |= x != 0.0f;
+  if (!any) return Status();
+  Plan plan;
+  Status s;
+  if (!(s = build_plan(root, p, plan)).ok()) return s;
+  if (plan.nslots > max_slots_) {
+    s.code = DCFR_ERR_INVALID_ARG;
+    s.msg = "subtree plan exceeds the reach buffer";
+    return s;
+  }
+  if (!(s = upload_plan(plan)).ok()) return s;
+  std::vector<float> row(stride_, 0.0f);
+  std::copy(opp_reach.begin(), opp_reach.end(), row.begin());
+  float* d_row = root_out_ + (size_t)(p ^ 1) * stride_;  // scratch row
+  CK(cudaMemcpyAsync(d_row, row.data(), stride_ * 4, cudaMemcpyHostToDevice, stream_));
+  enqueue_traversal(plan, M_AVG, d_row, nullptr);
+  launches += plan.kernels;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out.data(), vals_ + (size_t)root * stride_, (size_t)g.n[p] * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// query (lib.rs:842-899).
+Status Engine::query(const std::vector<dcfr_step>& path, dcfr_node_info& info, std::vector<Act>& actions,
+                     std::vector<uint16_t>& combos, std::vector<float>& strategy, std::vector<float>& ev,
+                     std::vector<float>& reach_real) {
+  uint32_t node;
+  std::vector<float> reach[2];
+  std::vector<uint32_t> to_canon[2];
+  Status s = walk(path, node, reach, to_canon);
+  if (!s.ok()) return s;
+  const GNode nd = g.nodes[node];
+  if (nd.kind != N_PLAYER) return bad_path("not a decision node");
+  const int q = nd.player, o = q ^ 1, n = g.n[q], na = nd.nchild;
+  // compatible_reach (hands.rs:102-125).
+  std::vector<double> compat(n);
+  {
+    double total = 0.0, minus[52] = {0};
+    for (int k = 0; k < g.n[o]; k++) {
+      float w = reach[o][k];
+      if (w != 0.0f) {
+        total += (double)w;
+        minus[g.c1[o][k]] += (double)w;
+        minus[g.c2[o][k]] += (double)w;
+      }
+    }
+    for (int i = 0; i < n; i++) {
+      double sw = g.same[q][i] == NO ? 0.0 : (double)reach[o][g.same[q][i]];
+      double v = total - minus[g.c1[q][i]] - minus[g.c2[q][i]] + sw;
+      compat[i] = v > 0.0 ? v : 0.0;
+    }
+  }
+  std::vector<std::vector<float>> child(na);
+  for (int a = 0; a < na; a++)
+    if (!(s = subtree_values(nd.first + a, q, reach[o], child[a])).ok()) return s;
+  const double offset = g.half_pot + (double)nd.invest[q];
+  std::vector<float> strat_c;
+  if (!(s = avg_strategy(node, strat_c)).ok()) return s;
+  ev.assign((size_t)na * n, 0.0f);
+  strategy.assign((size_t)na * n, 0.0f);
+  reach_real.assign(n, 0.0f);
+  for (int h = 0; h < n; h++) {
+    uint32_t hc = to_canon[q][h];
+    reach_real[h] = reach[q][hc];
+    double denom = compat[hc] * g.norm;
+    for (int a = 0; a < na; a++) {
+      strategy[(size_t)a * n + h] = strat_c[(size_t)a * n + hc];
+      ev[(size_t)a * n + h] = denom > 0.0 ? (float)((double)child[a][hc] / denom + offset) : 0.0f;
+    }
+  }
+  for (int p = 0; p < 2; p++) {
+    double root = -0.0, now = -0.0;
+    for (float x : g.weights[p]) root += (double)x;
+    for (float x : reach[p]) now += (double)x;
+    info.reach_fraction[p] = root > 0.0 ? now / root : 0.0;
+  }
+  info.player = q;
+  info.num_actions = na;
+  info.num_hands = n;
+  info.pot = g.cfg.root.pot + (int64_t)nd.invest[0] + (int64_t)nd.invest[1];
+  info.invest[0] = nd.invest[0];
+  info.invest[1] = nd.invest[1];
+  actions = g.actions(node);
+  combos = g.combos[q];
+  return Status();
+}
+
+// ranges_after (lib.rs:903-912).
+Status Engine::ranges_after(const std::vector<dcfr_step>& path, float out[2][DCFR_NUM_COMBOS]) {
+  uint32_t node;
+  std::vector<float> reach[2];
+  std::vector<uint32_t> to_canon[2];
+  Status s = walk(path, node, reach, to_canon);
+  if (!s.ok()) return s;
+  for (int p = 0; p < 2; p++) {
+    for (int c = 0; c < DCFR_NUM_COMBOS; c++) out[p][c] = 0.0f;
+    for (int h = 0; h < g.n[p]; h++) out[p][g.combos[p][h]] = reach[p][to_canon[p][h]];
+  }
+  return Status();
+}
+
+}  // namespace dcfr

@@ -1,0 +1,147 @@
+// Device engine of libdcfr: owns the device copy of the game, the storage,
+// the per-traversal plans and the captured CUDA graphs of one solver handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "game.hpp"
+#include "plan.hpp"
+
+namespace dcfr {
+
+struct RowArgs;
+struct TermArgs;
+
+// Kernel launchers (kernels.cu).
+void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s);
+void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s);
+void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, int ngroups, int blocks,
+                     cudaStream_t s);
+cudaError_t terminal_kernel_setup();
+size_t terminal_smem_bytes();
+void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,
+                     const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1, EntryD* out, uint32_t* count,
+                     int tstride, cudaStream_t s);
+void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
+void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
+void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
+
+// Status of a failed call: code + message.
+struct Status {
+  int code = DCFR_OK;
+  std::string msg;
+  bool ok() const { return code == DCFR_OK; }
+};
+
+// One traversal plan: traverser p over the subtree at `root`.
+struct Plan {
+  int p = 0;
+  uint32_t root = 0;
+  uint32_t nslots = 0;
+  struct Level {
+    uint32_t first = 0, count = 0;
+    int maxa = 0;
+  };
+  std::vector<Level> down, up;  // up[d] for depth d (launched deepest first)
+  std::vector<DownTask> h_down;
+  std::vector<UpTask> h_up;
+  std::vector<TermGroup> h_groups;
+  std::vector<TermLane> h_lanes;
+  DownTask* d_down = nullptr;
+  UpTask* d_up = nullptr;
+  TermGroup* d_groups = nullptr;
+  TermLane* d_lanes = nullptr;
+  int kernels = 0;  // kernel launches per traversal
+  uint64_t nodes = 0;
+  ~Plan();
+};
+
+class Engine {
+ public:
+  static Status create(const dcfr_config& cfg, std::unique_ptr<Engine>& out);
+  ~Engine();
+
+  Game g;
+  uint32_t iterations = 0;
+  double last_exploitability;
+  uint64_t launches = 0;
+  double last_iterate_ms = 0.0;
+
+  Status iterate(uint32_t n);
+  Status sync();
+  Status exploitability(double& out);
+  Status root_values(double out[2]);
+  Status traverse(int p, int mode, uint32_t t, float* out);
+  Status solve(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb, void* user,
+               dcfr_progress& out);
+  Status download(float* regrets, float* sums);
+  Status upload(const float* regrets, const float* sums);
+  Status set_iterations(uint32_t t);
+  Status query(const std::vector<dcfr_step>& path, dcfr_node_info& info, std::vector<Act>& actions,
+               std::vector<uint16_t>& combos, std::vector<float>& strategy, std::vector<float>& ev,
+               std::vector<float>& reach);
+  Status ranges_after(const std::vector<dcfr_step>& path, float out[2][DCFR_NUM_COMBOS]);
+  Status actions_at(const std::vector<dcfr_step>& path, std::vector<Act>& out, bool& decision);
+  double iteration_bytes() const;
+  int isomorphic_pairs() const;
+
+ private:
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  int hp_[2] = {0, 0};
+  int stride_ = 0;
+  std::vector<uint64_t> gpu_off_;  // per node: float offset of a player node's block
+  uint64_t gpu_len_ = 0;
+  // Device buffers.
+  float* regrets_ = nullptr;
+  float* sums_ = nullptr;
+  float* reach_ = nullptr;
+  float* vals_ = nullptr;
+  uint32_t* alive_ = nullptr;
+  float* root_rows_ = nullptr;   // [2][stride] opponent root weights per traverser
+  float* root_out_ = nullptr;    // [2][stride] root values after a traversal pair
+  uint8_t* hc1_[2] = {nullptr, nullptr};
+  uint8_t* hc2_[2] = {nullptr, nullptr};
+  uint32_t* same_[2] = {nullptr, nullptr};
+  uint16_t* perm_ = nullptr;
+  uint8_t* chance_cards_ = nullptr;
+  IsoRefD* iso_ = nullptr;
+  EntryD* tables_ = nullptr;
+  uint32_t* table_count_ = nullptr;
+  int tstride_ = 0;
+  double* scratch_ = nullptr;
+  int term_blocks_ = 0;
+  DiscountD* disc_table_ = nullptr;
+  uint32_t disc_len_ = 0;
+  DiscountD* cur_disc_ = nullptr;
+  uint32_t* counter_ = nullptr;
+  uint64_t max_slots_ = 0;
+  std::vector<uint32_t> cc_off_, iso_first_;
+  std::unique_ptr<Plan> full_[2];
+  cudaGraphExec_t iter_graph_ = nullptr, br_graph_ = nullptr, avg_graph_ = nullptr;
+  int iter_kernels_ = 0, pair_kernels_ = 0;
+
+  Status init();
+  Status build_plan(uint32_t root, int p, Plan& plan);
+  Status upload_plan(Plan& plan);
+  void row_args(int p, RowArgs& A) const;
+  void term_args(int p, TermArgs& A) const;
+  void enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out);
+  Status ensure_discounts(uint32_t max_t);
+  Status capture_graphs();
+  void free_graphs();
+  Status mode_root_values(int mode, double out[2]);
+  Status walk(const std::vector<dcfr_step>& path, uint32_t& node, std::vector<float> reach[2],
+              std::vector<uint32_t> to_canon[2]);
+  Status avg_strategy(uint32_t node, std::vector<float>& s);
+  Status subtree_values(uint32_t root, int p, const std::vector<float>& opp_reach, std::vector<float>& out);
+};
+
+Status cuda_status(cudaError_t e, const char* what);
+
+}  // namespace dcfr

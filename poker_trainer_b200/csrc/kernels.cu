@@ -1,0 +1,737 @@
+// sm_100a kernels of libdcfr.
+//
+// Every f32/f64 operation of the solve is performed in the order of the
+// reference CPU solver (AhanDatta/Poker-Trainer crates/solver/src/cfr.rs,
+// river.rs, eval.rs) and the library is compiled with -fmad=false, IEEE
+// division and denormals kept, so results are bit-identical to it:
+//   * row kernels (down_kernel / up_kernel) work on 4 hands per thread with
+//     128-bit loads and stores; all their arithmetic is per hand;
+//   * chance sums accumulate children in f64 in card order, then the
+//     isomorphic cards through the suit permutation (cfr.rs:462-478);
+//   * terminal values (terminal_kernel) run the reference's sequential
+//     strength-ordered sweeps (eval.rs:69-148, 214-344) in lockstep across the
+//     32 lanes of a warp, one terminal per lane, all lanes on the same board:
+//     the per-lane card-blocker sums live in shared memory ([52][32] f64), so
+//     every f64 sum is accumulated in the CPU's order.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.hpp"
+
+namespace dcfr {
+
+__device__ __forceinline__ float max0(float x) { return x > 0.0f ? x : 0.0f; }
+
+// recip (cfr.rs:114-121): 1/d for a positive d whose reciprocal is finite.
+__device__ __forceinline__ float recipf(float d) {
+  float i = 1.0f / d;
+  return (d > 0.0f && isfinite(i)) ? i : 0.0f;
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float& at(float4& v, int j) { return (&v.x)[j]; }
+__device__ __forceinline__ bool nz4(const float4& v) { return v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f; }
+
+// ------------------------------------------------------------- down levels
+// Opponent split (cfr.rs:384-420 / river.rs:115-160) and chance split
+// (cfr.rs:448-456).
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_THREADS) down_kernel(RowArgs A, const DownTask* __restrict__ tasks, int chunks) {
+  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
+  const DownTask T = tasks[t];
+  if (A.alive[T.in_slot] == 0) return;  // dead subtree: children stay dead
+  const int o = A.p ^ 1;
+  const int hp = A.hp[o];
+  const int h0 = ch * ROW_CHUNK + threadIdx.x * VEC;
+  const bool valid = h0 < hp;
+  const int lane = threadIdx.x & 31;
+  const size_t stride = (size_t)A.stride;
+  float4 r = valid ? ld4(A.reach + (size_t)T.in_slot * stride + h0) : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (T.kind == D_OPP_SPLIT) {
+    const int na = (int)T.nchild;
+    const float uniform = 1.0f / (float)na;
+    float4 x[MAXA];
+    float4 inv;
+    const float* base = (MODE == M_CFR ? A.regrets : A.sums) + T.store + h0;
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) x[a] = valid ? ld4(base + (size_t)a * hp) : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (MODE == M_CFR) {
+      // regret_match_into (cfr.rs:161-192).
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        float s = max0(at(x[0], j));
+#pragma unroll
+        for (int a = 1; a < MAXA; a++)
+          if (a < na) s += max0(at(x[a], j));
+        at(inv, j) = recipf(s);
+      }
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na)
+#pragma unroll
+          for (int j = 0; j < VEC; j++) at(x[a], j) = at(inv, j) == 0.0f ? uniform : max0(at(x[a], j)) * at(inv, j);
+      // Strategy sums s*gamma + sigma (or + sigma*reach) (cfr.rs:395-407).
+      const DiscountD d = *A.disc;
+      float* sb = A.sums + T.store + h0;
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na && valid) {
+          float4 s = ld4(sb + (size_t)a * hp);
+#pragma unroll
+          for (int j = 0; j < VEC; j++) {
+            float add = d.reach_weighted ? at(x[a], j) * at(r, j) : at(x[a], j);
+            at(s, j) = at(s, j) * d.strat + add;
+          }
+          st4(sb + (size_t)a * hp, s);
+        }
+    } else {
+      // normalize_in_place (cfr.rs:124-154).
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        float s = at(x[0], j);
+#pragma unroll
+        for (int a = 1; a < MAXA; a++)
+          if (a < na) s += at(x[a], j);
+        at(inv, j) = recipf(s);
+      }
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na)
+#pragma unroll
+          for (int j = 0; j < VEC; j++) at(x[a], j) = at(inv, j) == 0.0f ? uniform : at(x[a], j) * at(inv, j);
+    }
+    // Child reach = strategy * reach, and child liveness.
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) {
+        float4 c;
+#pragma unroll
+        for (int j = 0; j < VEC; j++) at(c, j) = at(x[a], j) * at(r, j);
+        if (valid) st4(A.reach + (size_t)(T.out_slot + a) * stride + h0, c);
+        bool any = __any_sync(0xffffffffu, valid && nz4(c));
+        if (any && lane == 0) A.alive[T.out_slot + a] = 1u;
+      }
+  } else {
+    // Chance split: reach*factor, opponent hands holding the card zeroed.
+    uchar4 oc1 = make_uchar4(255, 255, 255, 255), oc2 = oc1;
+    if (valid) {
+      oc1 = *reinterpret_cast<const uchar4*>(A.hc1[o] + h0);
+      oc2 = *reinterpret_cast<const uchar4*>(A.hc2[o] + h0);
+    }
+    const uint8_t* cards = A.chance_cards + T.cards;
+    for (uint32_t i = 0; i < T.nchild; i++) {
+      const uint8_t card = cards[i];
+      float4 c;
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        uint8_t a1 = (&oc1.x)[j], a2 = (&oc2.x)[j];
+        at(c, j) = (a1 == card || a2 == card) ? 0.0f : at(r, j) * T.factor;
+      }
+      if (valid) st4(A.reach + (size_t)(T.out_slot + i) * stride + h0, c);
+      bool any = __any_sync(0xffffffffu, valid && nz4(c));
+      if (any && lane == 0) A.alive[T.out_slot + i] = 1u;
+    }
+  }
+}
+
+// --------------------------------------------------------------- up levels
+// Traverser node (own_node_update, cfr.rs:315-382), opponent node sum
+// (cfr.rs:421-432, river.rs:264-271) and chance sum (cfr.rs:462-478).
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask* __restrict__ tasks, int chunks) {
+  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
+  const UpTask T = tasks[t];
+  if (A.alive[T.slot] == 0) return;
+  const int p = A.p;
+  const int hp = A.hp[p];
+  const int h0 = ch * ROW_CHUNK + threadIdx.x * VEC;
+  if (h0 >= hp) return;
+  const size_t stride = (size_t)A.stride;
+  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (T.kind == U_OWN) {
+    const int na = (int)T.nchild;
+    float4 cfv[MAXA];
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) cfv[a] = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
+    if (MODE == M_BR) {
+      out = cfv[0];
+#pragma unroll
+      for (int a = 1; a < MAXA; a++)
+        if (a < na)
+#pragma unroll
+          for (int j = 0; j < VEC; j++) at(out, j) = at(cfv[a], j) > at(out, j) ? at(cfv[a], j) : at(out, j);
+    } else if (MODE == M_AVG) {
+      float4 s[MAXA];
+      float4 inv;
+      const float uniform = 1.0f / (float)na;
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) s[a] = ld4(A.sums + T.store + (size_t)a * hp + h0);
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        float d = at(s[0], j);
+#pragma unroll
+        for (int a = 1; a < MAXA; a++)
+          if (a < na) d += at(s[a], j);
+        at(inv, j) = recipf(d);
+      }
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na)
+#pragma unroll
+          for (int j = 0; j < VEC; j++) {
+            float sv = at(inv, j) == 0.0f ? uniform : at(s[a], j) * at(inv, j);
+            at(out, j) += sv * at(cfv[a], j);
+          }
+    } else {
+      const DiscountD d = *A.disc;
+      float4 r[MAXA];
+      float4 inv;
+      float* rb = A.regrets + T.store + h0;
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) r[a] = ld4(rb + (size_t)a * hp);
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        float s = max0(at(r[0], j));
+#pragma unroll
+        for (int a = 1; a < MAXA; a++)
+          if (a < na) s += max0(at(r[a], j));
+        float o = 0.0f;
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na) o += max0(at(r[a], j)) * at(cfv[a], j);
+        float iv = recipf(s);
+        o *= iv;
+        if (iv == 0.0f) {
+          float m = -0.0f;
+#pragma unroll
+          for (int a = 0; a < MAXA; a++)
+            if (a < na) m += at(cfv[a], j);
+          o = m * (1.0f / (float)na);
+        }
+        at(out, j) = o;
+        at(inv, j) = iv;
+      }
+      (void)inv;
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) {
+#pragma unroll
+          for (int j = 0; j < VEC; j++) {
+            float x = at(r[a], j);
+            float disc = x > 0.0f ? d.pos : d.neg;
+            at(r[a], j) = x * disc + at(cfv[a], j) - at(out, j);
+          }
+          st4(rb + (size_t)a * hp, r[a]);
+        }
+    }
+  } else if (T.kind == U_OPP_SUM) {
+    for (uint32_t a = 0; a < T.nchild; a++) {
+      if (A.alive[T.child_slot + a] == 0) continue;
+      float4 v = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
+#pragma unroll
+      for (int j = 0; j < VEC; j++) at(out, j) += at(v, j);
+    }
+  } else {
+    double acc[VEC] = {0.0, 0.0, 0.0, 0.0};
+    const uchar4 mc1 = *reinterpret_cast<const uchar4*>(A.hc1[p] + h0);
+    const uchar4 mc2 = *reinterpret_cast<const uchar4*>(A.hc2[p] + h0);
+    const uint8_t* cards = A.chance_cards + T.cards;
+    for (uint32_t i = 0; i < T.nchild; i++) {
+      if (A.alive[T.child_slot + i] == 0) continue;
+      const uint8_t card = cards[i];
+      float4 v = ld4(A.vals + (size_t)(T.child + i) * stride + h0);
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        bool blocked = (&mc1.x)[j] == card || (&mc2.x)[j] == card;
+        acc[j] += blocked ? 0.0 : (double)at(v, j);
+      }
+    }
+    for (uint32_t k = 0; k < T.iso_count; k++) {
+      const IsoRefD ref = A.iso[T.iso_first + k];
+      if (A.alive[T.child_slot + ref.ci] == 0) continue;
+      const uint8_t card = cards[ref.ci];
+      const float* row = A.vals + (size_t)(T.child + ref.ci) * stride;
+      const uint16_t* perm = A.perm + (size_t)(p * 6 + ref.pair) * stride;
+#pragma unroll
+      for (int j = 0; j < VEC; j++) {
+        int h = h0 + j;
+        if (h < A.n[p]) {
+          int q = perm[h];
+          bool blocked = A.hc1[p][q] == card || A.hc2[p][q] == card;
+          acc[j] += blocked ? 0.0 : (double)row[q];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < VEC; j++) at(out, j) = (float)acc[j];
+  }
+  st4(A.vals + (size_t)T.node * stride + h0, out);
+}
+
+// ---------------------------------------------------------------- terminals
+__device__ __forceinline__ EntryD ld_entry(const EntryD* e) {
+  uint2 v = __ldg(reinterpret_cast<const uint2*>(e));
+  EntryD r;
+  r.strength = v.x;
+  r.idx = (uint16_t)(v.y & 0xFFFFu);
+  r.c1 = (uint8_t)((v.y >> 16) & 0xFFu);
+  r.c2 = (uint8_t)(v.y >> 24);
+  return r;
+}
+
+// Fold values for up to 32 fold terminals (one per lane): eval_fold
+// (eval.rs:40-64, kind T_FOLD_SCALAR) or fold_batch (eval.rs:173-206,
+// T_FOLD_BATCH); opponent sums in hand order.
+__device__ void fold_lanes(const TermArgs& A, uint32_t kind, bool live, const float* rr, float* orow, double pay,
+                           double (*mi)[32], int lane) {
+  const int p = A.p, o = p ^ 1;
+  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
+  double total = 0.0;
+  const uint8_t* oc1 = A.hc1[o];
+  const uint8_t* oc2 = A.hc2[o];
+  const int no = A.n[o];
+  for (int j = 0; j < no; j++) {
+    double w = live ? (double)rr[j] : 0.0;
+    total += w;
+    int a = __ldg(oc1 + j), b = __ldg(oc2 + j);
+    mi[a][lane] += w;
+    mi[b][lane] += w;
+  }
+  const int np = A.n[p], hp = A.hp[p];
+  const uint8_t* pc1 = A.hc1[p];
+  const uint8_t* pc2 = A.hc2[p];
+  const uint32_t* same = A.same[p];
+  for (int h = 0; h < hp; h++) {
+    float f = 0.0f;
+    if (h < np) {
+      double a = mi[__ldg(pc1 + h)][lane], b = mi[__ldg(pc2 + h)][lane];
+      uint32_t sm = __ldg(same + h);
+      double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
+      if (kind == T_FOLD_SCALAR)
+        f = total == 0.0 ? 0.0f : (float)(pay * ((total - (a + b)) + sw));
+      else
+        f = (float)(pay * (((total - a) - b) + sw));
+    }
+    if (live) orow[h] = f;
+  }
+}
+
+// Showdown values for up to 32 showdown terminals on one board: eval_showdown
+// (eval.rs:69-148, T_SHOWDOWN_SCALAR) or showdown_batch (eval.rs:214-344,
+// T_SHOWDOWN_BATCH, with the paired fold read off the ascending sweep).
+__device__ void showdown_lanes(const TermArgs& A, const TermGroup& G, const TermLane& L, bool live, const float* rr,
+                               float* orow, double (*mi)[32], double* scr, int lane) {
+  const int p = A.p, o = p ^ 1;
+  const EntryD* mine = A.tables + (size_t)(G.board * 2 + p) * A.tstride;
+  const EntryD* theirs = A.tables + (size_t)(G.board * 2 + o) * A.tstride;
+  const int cm = (int)A.table_count[G.board * 2 + p];
+  const int ct = (int)A.table_count[G.board * 2 + o];
+  const bool batch = G.kind == T_SHOWDOWN_BATCH;
+  const int hp = A.hp[p];
+  // Zero the rows of live lanes (hands blocked by the board stay 0).
+  unsigned lm = __ballot_sync(0xffffffffu, live);
+  while (lm) {
+    int t = __ffs(lm) - 1;
+    lm &= lm - 1;
+    uint32_t row = __shfl_sync(0xffffffffu, L.row, t);
+    float* r = A.vals + (size_t)row * A.stride;
+    for (int h = lane * VEC; h < hp; h += 32 * VEC) st4(r + h, make_float4(0.f, 0.f, 0.f, 0.f));
+  }
+  __syncwarp();
+  // Pass 1, ascending: opponent hands strictly weaker.
+  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
+  double sum = 0.0;
+  int i = 0, j = 0;
+  while (i < cm) {
+    const uint32_t s = ld_entry(mine + i).strength;
+    while (j < ct) {
+      EntryD e = ld_entry(theirs + j);
+      if (e.strength >= s) break;
+      double w = live ? (double)rr[e.idx] : 0.0;
+      sum += w;
+      mi[e.c1][lane] += w;
+      mi[e.c2][lane] += w;
+      j++;
+    }
+    while (i < cm) {
+      EntryD e = ld_entry(mine + i);
+      if (e.strength != s) break;
+      double a = mi[e.c1][lane], b = mi[e.c2][lane];
+      scr[(size_t)i * 32 + lane] = batch ? L.a * ((sum - a) - b) : L.a * (sum - (a + b));
+      i++;
+    }
+  }
+  // Paired fold: finish the sweep and read the fold off the sums.
+  const bool has_fold = batch && live && L.frow != NONE32;
+  if (__any_sync(0xffffffffu, has_fold)) {
+    while (j < ct) {
+      EntryD e = ld_entry(theirs + j);
+      double w = live ? (double)rr[e.idx] : 0.0;
+      sum += w;
+      mi[e.c1][lane] += w;
+      mi[e.c2][lane] += w;
+      j++;
+    }
+    float* frow = A.vals + (size_t)(has_fold ? L.frow : 0) * A.stride;
+    const int np = A.n[p];
+    for (int h = 0; h < hp; h++) {
+      float f = 0.0f;
+      if (h < np) {
+        double a = mi[__ldg(A.hc1[p] + h)][lane], b = mi[__ldg(A.hc2[p] + h)][lane];
+        uint32_t sm = __ldg(A.same[p] + h);
+        double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
+        f = (float)(L.d * (((sum - a) - b) + sw));
+      }
+      if (has_fold) frow[h] = f;
+    }
+  }
+  // Pass 2, descending: opponent hands strictly stronger.
+  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
+  sum = 0.0;
+  i = cm;
+  j = ct;
+  while (i > 0) {
+    const uint32_t s = ld_entry(mine + i - 1).strength;
+    while (j > 0) {
+      EntryD e = ld_entry(theirs + j - 1);
+      if (e.strength <= s) break;
+      double w = live ? (double)rr[e.idx] : 0.0;
+      sum += w;
+      mi[e.c1][lane] += w;
+      mi[e.c2][lane] += w;
+      j--;
+    }
+    while (i > 0) {
+      EntryD e = ld_entry(mine + i - 1);
+      if (e.strength != s) break;
+      double a = mi[e.c1][lane], b = mi[e.c2][lane];
+      double W = scr[(size_t)(i - 1) * 32 + lane];
+      float v;
+      if (batch)
+        v = (float)(W + L.b * ((sum - a) - b));
+      else
+        v = (float)W + (float)(L.b * (sum - (a + b)));
+      if (live) orow[e.idx] = v;
+      i--;
+    }
+  }
+  // Ties (add_ties, eval.rs:347-379) when the tie payoff is nonzero.
+  const bool tie = live && L.c != 0.0;
+  if (__any_sync(0xffffffffu, tie)) {
+    for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
+    int k = 0;
+    j = 0;
+    while (k < cm) {
+      const uint32_t s = ld_entry(mine + k).strength;
+      while (j < ct && ld_entry(theirs + j).strength < s) j++;
+      double eq_sum = 0.0;
+      int jj = j;
+      while (jj < ct) {
+        EntryD e = ld_entry(theirs + jj);
+        if (e.strength != s) break;
+        double w = live ? (double)rr[e.idx] : 0.0;
+        eq_sum += w;
+        mi[e.c1][lane] += w;
+        mi[e.c2][lane] += w;
+        jj++;
+      }
+      while (k < cm) {
+        EntryD e = ld_entry(mine + k);
+        if (e.strength != s) break;
+        uint32_t sm = __ldg(A.same[p] + e.idx);
+        double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
+        double eq = (eq_sum - (mi[e.c1][lane] + mi[e.c2][lane])) + sw;
+        if (tie) orow[e.idx] += (float)(L.c * eq);
+        k++;
+      }
+      for (int q = j; q < jj; q++) {
+        EntryD e = ld_entry(theirs + q);
+        mi[e.c1][lane] = 0.0;
+        mi[e.c2][lane] = 0.0;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TERM_WARPS * 32) terminal_kernel(TermArgs A, const TermGroup* __restrict__ groups,
+                                                                    const TermLane* __restrict__ lanes, int ngroups) {
+  extern __shared__ double smem_minus[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double(*mi)[32] = reinterpret_cast<double(*)[32]>(smem_minus + (size_t)warp * 52 * 32);
+  const int gw = blockIdx.x * TERM_WARPS + warp;
+  const int nw = gridDim.x * TERM_WARPS;
+  double* scr = A.scratch + (size_t)gw * A.nmax * 32;
+  for (int g = gw; g < ngroups; g += nw) {
+    const TermGroup G = groups[g];
+    const bool act = lane < (int)G.count;
+    TermLane L;
+    if (act) {
+      L = lanes[G.first + lane];
+    } else {
+      L.slot = 0;
+      L.row = 0;
+      L.frow = NONE32;
+      L.pad = 0;
+      L.a = L.b = L.c = L.d = 0.0;
+    }
+    const bool live = act && A.alive[L.slot] != 0;
+    const float* rr = A.reach + (size_t)L.slot * A.stride;
+    float* orow = A.vals + (size_t)L.row * A.stride;
+    if (G.kind == T_FOLD_SCALAR || G.kind == T_FOLD_BATCH)
+      fold_lanes(A, G.kind, live, rr, orow, L.a, mi, lane);
+    else
+      showdown_lanes(A, G, L, live, rr, orow, mi, scr, lane);
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ setup kernels
+// 7-card strength (crates/holdem/src/eval.rs:104-198): category<<26 | payload.
+__device__ __forceinline__ uint32_t hb(uint32_t x) { return 31u - (uint32_t)__clz(x); }
+
+__device__ uint32_t topb(uint32_t x, uint32_t n) {
+  uint32_t out = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    if (x == 0) break;
+    uint32_t b = 1u << hb(x);
+    out |= b;
+    x ^= b;
+  }
+  return out;
+}
+
+__device__ int straight_top(uint32_t ranks) {
+  uint32_t run = ranks & (ranks << 1) & (ranks << 2) & (ranks << 3) & (ranks << 4);
+  if (run) return (int)hb(run);
+  if ((ranks & 0x100Fu) == 0x100Fu) return 3;
+  return -1;
+}
+
+__device__ uint32_t strength_of(uint64_t mask) {
+  uint32_t s[4] = {(uint32_t)(mask & 0x1FFF), (uint32_t)((mask >> 16) & 0x1FFF), (uint32_t)((mask >> 32) & 0x1FFF),
+                   (uint32_t)((mask >> 48) & 0x1FFF)};
+  for (int k = 0; k < 4; k++)
+    if (__popc(s[k]) >= 5) {
+      int h = straight_top(s[k]);
+      return h >= 0 ? (8u << 26) | (uint32_t)h : (5u << 26) | topb(s[k], 5);
+    }
+  uint32_t any = s[0] | s[1] | s[2] | s[3];
+  uint32_t two = (s[0] & s[1]) | (s[0] & s[2]) | (s[0] & s[3]) | (s[1] & s[2]) | (s[1] & s[3]) | (s[2] & s[3]);
+  uint32_t three = (s[0] & s[1] & s[2]) | (s[0] & s[1] & s[3]) | (s[0] & s[2] & s[3]) | (s[1] & s[2] & s[3]);
+  uint32_t four = s[0] & s[1] & s[2] & s[3];
+  if (four) {
+    uint32_t q = hb(four);
+    return (7u << 26) | (q << 13) | topb(any & ~(1u << q), 1);
+  }
+  if (three) {
+    uint32_t t = hb(three);
+    uint32_t rest = two & ~(1u << t);
+    if (rest) return (6u << 26) | (t << 13) | (1u << hb(rest));
+  }
+  int h = straight_top(any);
+  if (h >= 0) return (4u << 26) | (uint32_t)h;
+  if (three) {
+    uint32_t t = hb(three);
+    return (3u << 26) | (t << 13) | topb(any & ~(1u << t), 2);
+  }
+  if (__popc(two) >= 2) {
+    uint32_t pairs = topb(two, 2);
+    return (2u << 26) | (pairs << 13) | topb(any & ~pairs, 1);
+  }
+  if (two) {
+    uint32_t pp = hb(two);
+    return (1u << 26) | (pp << 13) | topb(any & ~(1u << pp), 3);
+  }
+  return topb(any, 5);
+}
+
+__device__ __forceinline__ uint64_t lane_bit(int c) { return 1ull << ((c & 3) * 16 + (c >> 2)); }
+
+// One block per (board, player): strengths of the player's hands that don't
+// touch the board, sorted by (strength, hand index) — StrengthTable::new
+// (crates/solver/src/hands.rs:137-158).
+constexpr int SORT_N = 2048;
+__global__ void __launch_bounds__(512) strength_kernel(const uint8_t* __restrict__ boards, const uint8_t* hc1_0,
+                                                       const uint8_t* hc2_0, const uint8_t* hc1_1,
+                                                       const uint8_t* hc2_1, int n0, int n1, EntryD* out,
+                                                       uint32_t* count, int tstride) {
+  __shared__ unsigned long long keys[SORT_N];
+  const int b = blockIdx.x >> 1, q = blockIdx.x & 1;
+  const uint8_t* c1 = q ? hc1_1 : hc1_0;
+  const uint8_t* c2 = q ? hc2_1 : hc2_0;
+  const int n = q ? n1 : n0;
+  uint64_t mask = 0, set = 0;
+  for (int k = 0; k < 5; k++) {
+    int c = boards[b * 5 + k];
+    mask |= lane_bit(c);
+    set |= 1ull << c;
+  }
+  int valid_local = 0;
+  for (int i = threadIdx.x; i < SORT_N; i += blockDim.x) {
+    unsigned long long key = ~0ull;
+    if (i < n) {
+      int a = c1[i], bb = c2[i];
+      if (!((set >> a) & 1) && !((set >> bb) & 1)) {
+        uint32_t st = strength_of(mask | lane_bit(a) | lane_bit(bb));
+        key = ((unsigned long long)st << 32) | ((unsigned long long)i << 16) | ((unsigned long long)a << 8) |
+              (unsigned long long)bb;
+        valid_local++;
+      }
+    }
+    keys[i] = key;
+  }
+  __syncthreads();
+  // Bitonic sort, ascending.
+  for (int k = 2; k <= SORT_N; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int i = threadIdx.x; i < SORT_N; i += blockDim.x) {
+        int ixj = i ^ jj;
+        if (ixj > i) {
+          unsigned long long x = keys[i], y = keys[ixj];
+          bool up = (i & k) == 0;
+          if ((x > y) == up) {
+            keys[i] = y;
+            keys[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __shared__ int total;
+  if (threadIdx.x == 0) total = 0;
+  __syncthreads();
+  atomicAdd(&total, valid_local);
+  __syncthreads();
+  const int cnt = total;
+  EntryD* dst = out + (size_t)blockIdx.x * tstride;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    unsigned long long k = keys[i];
+    EntryD e;
+    e.strength = (uint32_t)(k >> 32);
+    e.idx = (uint16_t)((k >> 16) & 0xFFFF);
+    e.c1 = (uint8_t)((k >> 8) & 0xFF);
+    e.c2 = (uint8_t)(k & 0xFF);
+    dst[i] = e;
+  }
+  if (threadIdx.x == 0) count[blockIdx.x] = (uint32_t)cnt;
+}
+
+// Strengths of explicit 5..7-card hands given as eval lane masks (tests of
+// the device evaluator against the reference's).
+__global__ void evaluate_kernel(const unsigned long long* masks, uint32_t* out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = strength_of(masks[i]);
+}
+
+// All 2,598,960 five-card hands, per-category counts (eval.rs:246-265).
+__global__ void five_card_counts_kernel(unsigned long long* counts) {
+  __shared__ unsigned int local[9];
+  if (threadIdx.x < 9) local[threadIdx.x] = 0;
+  __syncthreads();
+  // blockIdx.x enumerates (a, b) pairs; threads enumerate (c, d, e).
+  int a = 0, b = 0, idx = blockIdx.x;
+  for (a = 0; a < 52; a++) {
+    int nb = 51 - a;
+    if (idx < nb) {
+      b = a + 1 + idx;
+      break;
+    }
+    idx -= nb;
+  }
+  uint64_t m2 = lane_bit(a) | lane_bit(b);
+  for (int t = threadIdx.x; t < 52 * 52; t += blockDim.x) {
+    int c = t / 52, d = t % 52;
+    if (c <= b || d <= c) continue;
+    uint64_t m4 = m2 | lane_bit(c) | lane_bit(d);
+    for (int e = d + 1; e < 52; e++) atomicAdd(&local[strength_of(m4 | lane_bit(e)) >> 26], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) atomicAdd(&counts[threadIdx.x], (unsigned long long)local[threadIdx.x]);
+}
+
+// Iteration counter: t += 1 and the iteration's discounts from the table.
+__global__ void advance_kernel(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur) {
+  uint32_t t = *counter + 1;
+  *counter = t;
+  *cur = table[t < table_len ? t : table_len - 1];
+}
+
+// ---------------------------------------------------------- host launchers
+template <int MODE, int MAXA>
+static void launch_down_t(const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s) {
+  down_kernel<MODE, MAXA><<<ntasks * chunks, ROW_THREADS, 0, s>>>(A, tasks, chunks);
+}
+template <int MODE, int MAXA>
+static void launch_up_t(const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s) {
+  up_kernel<MODE, MAXA><<<ntasks * chunks, ROW_THREADS, 0, s>>>(A, tasks, chunks);
+}
+
+void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s) {
+  if (maxa <= 4) {
+    if (mode == M_CFR) launch_down_t<M_CFR, 4>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_down_t<M_BR, 4>(A, tasks, ntasks, chunks, s);
+    else launch_down_t<M_AVG, 4>(A, tasks, ntasks, chunks, s);
+  } else if (maxa <= 8) {
+    if (mode == M_CFR) launch_down_t<M_CFR, 8>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_down_t<M_BR, 8>(A, tasks, ntasks, chunks, s);
+    else launch_down_t<M_AVG, 8>(A, tasks, ntasks, chunks, s);
+  } else {
+    if (mode == M_CFR) launch_down_t<M_CFR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_down_t<M_BR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+    else launch_down_t<M_AVG, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+  }
+}
+
+void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s) {
+  if (maxa <= 4) {
+    if (mode == M_CFR) launch_up_t<M_CFR, 4>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_up_t<M_BR, 4>(A, tasks, ntasks, chunks, s);
+    else launch_up_t<M_AVG, 4>(A, tasks, ntasks, chunks, s);
+  } else if (maxa <= 8) {
+    if (mode == M_CFR) launch_up_t<M_CFR, 8>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_up_t<M_BR, 8>(A, tasks, ntasks, chunks, s);
+    else launch_up_t<M_AVG, 8>(A, tasks, ntasks, chunks, s);
+  } else {
+    if (mode == M_CFR) launch_up_t<M_CFR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+    else if (mode == M_BR) launch_up_t<M_BR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+    else launch_up_t<M_AVG, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+  }
+}
+
+size_t terminal_smem_bytes() { return (size_t)TERM_WARPS * 52 * 32 * sizeof(double); }
+
+cudaError_t terminal_kernel_setup() {
+  return cudaFuncSetAttribute(terminal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)terminal_smem_bytes());
+}
+
+void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, int ngroups, int blocks,
+                     cudaStream_t s) {
+  terminal_kernel<<<blocks, TERM_WARPS * 32, terminal_smem_bytes(), s>>>(A, groups, lanes, ngroups);
+}
+
+void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,
+                     const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1, EntryD* out, uint32_t* count,
+                     int tstride, cudaStream_t s) {
+  strength_kernel<<<nboards * 2, 512, 0, s>>>(boards, hc1_0, hc2_0, hc1_1, hc2_1, n0, n1, out, count, tstride);
+}
+
+void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s) {
+  evaluate_kernel<<<(n + 255) / 256, 256, 0, s>>>(masks, out, n);
+}
+
+void launch_five_card_counts(unsigned long long* counts, cudaStream_t s) {
+  five_card_counts_kernel<<<52 * 51 / 2, 256, 0, s>>>(counts);
+}
+
+void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s) {
+  advance_kernel<<<1, 1, 0, s>>>(counter, table, table_len, cur);
+}
+
+}  // namespace dcfr

@@ -1,0 +1,131 @@
+// Device plan of one traversal: POD task records shared by the host planner
+// (engine.cu) and the kernels (kernels.cu).
+//
+// A traversal for traverser p over a subtree is level-synchronous:
+//   down levels  — opponent nodes split the opponent reach by their
+//                  strategy (regret matching + strategy-sum update in CFR
+//                  mode), chance nodes fan the reach out per dealt card;
+//   terminals    — fold and showdown values of every live terminal, one
+//                  warp per group of up to 32 terminals;
+//   up levels    — deepest first: traverser nodes combine child values
+//                  (and update regrets), opponent nodes and chance nodes sum.
+// Reach rows live in "slots" (a traverser node's children share its slot);
+// value rows are indexed by node id. Every row has HP floats (hands padded
+// to a multiple of 8, padding kept at zero).
+#pragma once
+
+#include <cstdint>
+
+namespace dcfr {
+
+constexpr int VEC = 4;             // hands per thread in the row kernels (float4)
+constexpr int ROW_THREADS = 128;   // threads per row-kernel block
+constexpr int ROW_CHUNK = VEC * ROW_THREADS;
+constexpr int MAX_ACTIONS = 16;
+constexpr int TERM_WARPS = 4;      // warps per terminal-kernel block
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+
+enum DownKind : uint32_t { D_OPP_SPLIT = 0, D_CHANCE_SPLIT = 1 };
+enum UpKind : uint32_t { U_OWN = 0, U_OPP_SUM = 1, U_CHANCE_SUM = 2 };
+enum TermKind : uint32_t { T_FOLD_SCALAR = 0, T_FOLD_BATCH = 1, T_SHOWDOWN_SCALAR = 2, T_SHOWDOWN_BATCH = 3 };
+enum ModeId : int { M_CFR = 0, M_BR = 1, M_AVG = 2 };
+
+struct DownTask {
+  uint32_t kind;
+  uint32_t in_slot;   // reach slot of the node
+  uint32_t out_slot;  // slot of the first child (children's slots are consecutive)
+  uint32_t nchild;
+  uint64_t store;     // opponent split: float offset of the node's block
+  uint32_t cards;     // chance split: offset of the children's cards in chance_cards
+  float factor;       // chance split: reach multiplier
+};
+
+struct UpTask {
+  uint32_t kind;
+  uint32_t slot;        // reach slot of the node (liveness)
+  uint32_t node;        // value row
+  uint32_t child;       // first child's node id (value rows are consecutive)
+  uint32_t nchild;
+  uint32_t child_slot;  // first child's slot (opponent / chance nodes)
+  uint64_t store;       // traverser node: float offset of its block
+  uint32_t cards;       // chance: offset of the children's cards
+  uint32_t iso_first;   // chance: first isomorphic reference
+  uint32_t iso_count;
+  uint32_t pad;
+};
+
+struct IsoRefD {
+  uint16_t ci;    // canonical child index
+  uint8_t pair;   // suit pair (0..5)
+  uint8_t pad;
+};
+
+struct TermLane {
+  uint32_t slot;  // reach slot
+  uint32_t row;   // value row (node id)
+  uint32_t frow;  // paired fold's value row, or NONE32
+  uint32_t pad;
+  double a;       // fold payoff / showdown win
+  double b;       // showdown lose
+  double c;       // showdown tie
+  double d;       // paired fold payoff
+};
+
+struct TermGroup {
+  uint32_t kind;
+  uint32_t board;  // showdown strength table
+  uint32_t first;  // first lane in the lane array
+  uint32_t count;  // lanes used (1..32)
+};
+
+// Strength-table entry (eval::Entry, crates/solver/src/eval.rs:11-18).
+struct EntryD {
+  uint32_t strength;
+  uint16_t idx;
+  uint8_t c1, c2;
+};
+
+struct DiscountD {
+  float pos, neg, strat;
+  int reach_weighted;
+};
+
+// Arguments of the row kernels (down/up levels) of one traversal.
+struct RowArgs {
+  float* regrets;
+  float* sums;
+  float* reach;
+  float* vals;
+  uint32_t* alive;
+  const uint8_t* hc1[2];  // hand cards, padded to hp with 255
+  const uint8_t* hc2[2];
+  const uint16_t* perm;   // [(q*6+pair)*stride + h]
+  const uint8_t* chance_cards;
+  const IsoRefD* iso;
+  const DiscountD* disc;
+  int n[2];
+  int hp[2];
+  int stride;
+  int p;
+};
+
+// Arguments of the terminal kernel.
+struct TermArgs {
+  const float* reach;
+  float* vals;
+  const uint32_t* alive;
+  double* scratch;  // [warps][nmax][32]
+  const EntryD* tables;
+  const uint32_t* table_count;
+  const uint8_t* hc1[2];
+  const uint8_t* hc2[2];
+  const uint32_t* same[2];
+  int n[2];
+  int hp[2];
+  int stride;
+  int tstride;
+  int nmax;
+  int p;
+};
+
+}  // namespace dcfr

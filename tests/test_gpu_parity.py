@@ -1,0 +1,142 @@
+"""GPU parity against the CPU oracle (the C++ restatement of the reference's
+CPU DCFR solver). The GPU path performs the reference's floating-point
+operations in the reference's order, so the bar is bit-identical results:
+root values of single traversals, regrets and strategy sums after
+iterations, exploitability, and queries. The reference's own GPU-vs-CPU
+standard (crates/solver/src/gpu/engine/tests.rs:729-754, "exact mode
+bit-identical to the CPU") is the one applied here."""
+import numpy as np
+import pytest
+
+import spots
+from oracle_api import OracleSolver
+from poker_trainer_b200 import abi, workloads
+from poker_trainer_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+SPOTS = {
+    "river": spots.river_config,
+    "turn": spots.turn_config,
+    "iso_turn": spots.iso_turn_config,
+    "allin_turn": spots.allin_turn_config,
+    "mid_street_raked": lambda: spots.mid_street_config(True),
+    "mid_street": lambda: spots.mid_street_config(False),
+}
+
+
+def bits(a):
+    return np.asarray(a, np.float32).view(np.uint32)
+
+
+def assert_bit_equal(a, b, what):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    assert a.shape == b.shape, what
+    diff = np.nonzero(bits(a) != bits(b))[0]
+    # -0.0 and +0.0 are the same value.
+    diff = [i for i in diff if not (a[i] == 0.0 and b[i] == 0.0)]
+    if diff:
+        i = diff[0]
+        pytest.fail(f"{what}: {len(diff)} of {len(a)} differ; first at {i}: gpu {a[i]!r} oracle {b[i]!r}")
+
+
+def random_storage(n, seed):
+    rng = np.random.default_rng(seed)
+    r = (rng.standard_normal(n) * 50).astype(np.float32)
+    r[rng.random(n) < 0.3] = 0.0
+    s = (rng.random(n) * 10).astype(np.float32)
+    s[rng.random(n) < 0.2] = 0.0
+    return r, s
+
+
+@pytest.mark.parametrize("name", list(SPOTS))
+def test_traversal_values_bit_identical(gpu, name):
+    cfg = SPOTS[name]()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    assert g.storage_len() == len(o.storage()[0])
+    r, s = random_storage(g.storage_len(), 7)
+    for p in (0, 1):
+        for mode in (abi.MODE_BEST_RESPONSE, abi.MODE_AVERAGE, abi.MODE_CFR):
+            o.set_storage(r, s)
+            g.upload_storage(r, s)
+            vo = o.traverse(p, mode, 5)
+            vg = g.traverse(p, mode, 5)
+            assert_bit_equal(vg, vo, f"{name} p={p} mode={mode} values")
+            if mode == abi.MODE_CFR:
+                ro, so = o.storage()
+                rg, sg = g.download_storage()
+                assert_bit_equal(rg, ro, f"{name} p={p} regrets")
+                assert_bit_equal(sg, so, f"{name} p={p} strategy sums")
+
+
+@pytest.mark.parametrize("name", list(SPOTS))
+def test_five_iterations_bit_identical(gpu, name):
+    cfg = SPOTS[name]()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(5)
+    g.iterate(5)
+    ro, so = o.storage()
+    rg, sg = g.download_storage()
+    assert_bit_equal(rg, ro, f"{name} regrets")
+    assert_bit_equal(sg, so, f"{name} sums")
+    assert g.exploitability() == o.exploitability()
+    assert np.array_equal(g.root_values(), o.root_values())
+
+
+def test_river_workload_1000_iterations_bit_identical(gpu):
+    """The river workload (Ks7s2dTh4c, 1000 iterations) end to end."""
+    cfg = workloads.river_spot()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(1000)
+    g.iterate(1000)
+    ro, so = o.storage()
+    rg, sg = g.download_storage()
+    assert_bit_equal(rg, ro, "regrets")
+    assert_bit_equal(sg, so, "sums")
+    assert g.exploitability() == o.exploitability()
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_random_river_spots_bit_identical(gpu, seed):
+    cfg = spots.random_river_config(seed)
+    try:
+        o = OracleSolver(cfg)
+    except Exception:
+        pytest.skip("spot rejected by Solver::new")
+    g = Solver.new(cfg)
+    o.iterate(6)
+    g.iterate(6)
+    ro, so = o.storage()
+    rg, sg = g.download_storage()
+    assert_bit_equal(rg, ro, "regrets")
+    assert_bit_equal(sg, so, "sums")
+    assert g.exploitability() == o.exploitability()
+
+
+@pytest.mark.parametrize("name", ["river", "iso_turn", "mid_street_raked"])
+def test_queries_match(gpu, name):
+    cfg = SPOTS[name]()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(8)
+    g.iterate(8)
+    paths = [[]]
+    acts = o.actions_at([])
+    paths.append([acts[-1]])
+    if name == "iso_turn":
+        paths += [["check", "check", "7c"], ["check", "check", "7h"], ["check", "check", "As"]]
+    for path in paths:
+        qo = o.query(path)
+        qg = g.query(path)
+        assert qg.actions == qo["actions"]
+        assert np.array_equal(qg.combos, qo["combos"])
+        assert_bit_equal(qg.strategy.ravel(), qo["strategy"].ravel(), f"{path} strategy")
+        assert_bit_equal(qg.ev.ravel(), qo["ev"].ravel(), f"{path} ev")
+        assert_bit_equal(qg.reach, qo["reach"], f"{path} reach")
+        ra = g.ranges_after(path)
+        rb = o.ranges_after(path)
+        assert_bit_equal(ra.ravel(), rb.ravel(), f"{path} ranges")
