@@ -51,6 +51,7 @@ Plan::~Plan() {
   dfree(d_up);
   dfree(d_groups);
   dfree(d_lanes);
+  dfree(d_tasks);
 }
 
 // DcfrParams -> Discount (cfr.rs:86-106), host f64 pow as the reference.
@@ -125,7 +126,16 @@ Engine::~Engine() {
   dfree(iso_);
   dfree(tables_);
   dfree(table_count_);
-  dfree(scratch_);
+  dfree(progs_);
+  dfree(prog_count_);
+  dfree(posmap_);
+  for (int q = 0; q < 2; q++) {
+    dfree(fold_prog_[q]);
+    dfree(emit_rec_[q]);
+  }
+  dfree(warp_scratch_);
+  dfree(group_scratch_);
+  dfree(counters_);
   dfree(disc_table_);
   dfree(cur_disc_);
   dfree(counter_);
@@ -187,6 +197,8 @@ Status Engine::init() {
   CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
   CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
 
+  tstride_ = std::max(g.n[0], g.n[1]);
+  pstride_ = (2 * tstride_ + TERM_CHUNK - 1) / TERM_CHUNK * TERM_CHUNK;
   // Hands.
   for (int q = 0; q < 2; q++) {
     std::vector<uint8_t> a(hp_[q], 255), b(hp_[q], 255);
@@ -202,6 +214,13 @@ Status Engine::init() {
     CK(cudaMemcpy(hc1_[q], a.data(), hp_[q], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(hc2_[q], b.data(), hp_[q], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(same_[q], sm.data(), hp_[q] * 4, cudaMemcpyHostToDevice));
+    // The player's hands in hand order as sweep steps (fold sums) and per-hand
+    // emit records (terminal.cu).
+    const int npad = (g.n[q] + TERM_CHUNK - 1) / TERM_CHUNK * TERM_CHUNK;
+    if (!(s = dalloc(fold_prog_[q], npad, "hands")).ok()) return s;
+    if (!(s = dalloc(emit_rec_[q], g.n[q], "hands")).ok()) return s;
+    launch_hand_program(hc1_[q], hc2_[q], same_[q], g.n[q], npad, fold_prog_[q], emit_rec_[q], stream_);
+    CK(cudaGetLastError());
   }
   {
     std::vector<uint16_t> perm((size_t)12 * stride_, 0);
@@ -234,7 +253,6 @@ Status Engine::init() {
   // Strength tables, built on the device.
   {
     const int nb = (int)g.boards.size();
-    tstride_ = std::max(g.n[0], g.n[1]);
     if (!(s = dalloc(tables_, (size_t)std::max(nb, 1) * 2 * tstride_, "strength tables")).ok()) return s;
     if (!(s = dalloc(table_count_, (size_t)std::max(nb, 1) * 2, "strength tables")).ok()) return s;
     if (nb > 0) {
@@ -246,6 +264,12 @@ Status Engine::init() {
       CK(cudaMemcpy(d_boards, bc.data(), bc.size(), cudaMemcpyHostToDevice));
       launch_strength(d_boards, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1], tables_, table_count_,
                       tstride_, stream_);
+      CK(cudaGetLastError());
+      // Sweep programs (terminal.cu): per board, traverser and pass.
+      if (!(s = dalloc(progs_, (size_t)nb * 6 * pstride_, "sweep programs")).ok()) return s;
+      if (!(s = dalloc(prog_count_, (size_t)nb * 6, "sweep programs")).ok()) return s;
+      if (!(s = dalloc(posmap_, (size_t)nb * 6 * tstride_, "sweep programs")).ok()) return s;
+      launch_programs(tables_, table_count_, tstride_, progs_, prog_count_, posmap_, pstride_, nb, stream_);
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(stream_));
       cudaFree(d_boards);
@@ -271,14 +295,20 @@ Status Engine::init() {
     CK(cudaMemcpy(root_rows_, rr.data(), rr.size() * 4, cudaMemcpyHostToDevice));
     if (!(s = dalloc(root_out_, rr.size(), "root rows")).ok()) return s;
   }
-  // Terminal scratch: one [nmax][32] f64 block per resident warp.
+  // Terminal scratch, sized for the largest terminal launch of the two plans.
   {
-    int dev = 0, sms = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    term_blocks_ = sms * 2;
-    if (!(s = dalloc(scratch_, (size_t)term_blocks_ * TERM_WARPS * tstride_ * 32, "terminal scratch")).ok())
+    for (int p = 0; p < 2; p++)
+      for (const Plan::Wave& w : full_[p]->waves) {
+        wave_tasks_ = std::max<int>(wave_tasks_, (int)w.count);
+        wave_groups_ = std::max<int>(wave_groups_, (int)w.groups);
+      }
+    warp_scratch_floats_ = (size_t)(pstride_ + 1) * 32 + (size_t)stride_ * 32;
+    if (!(s = dalloc(warp_scratch_, (size_t)std::max(wave_tasks_, 1) * warp_scratch_floats_, "terminal scratch")).ok())
       return s;
+    if (!(s = dalloc(group_scratch_, (size_t)std::max(wave_groups_, 1) * 2 * tstride_ * 32, "terminal scratch")).ok())
+      return s;
+    if (!(s = dalloc(counters_, (size_t)std::max(wave_groups_, 1), "terminal scratch")).ok()) return s;
+    CK(cudaMemsetAsync(counters_, 0, (size_t)std::max(wave_groups_, 1) * 4, stream_));
   }
   for (int p = 0; p < 2; p++)
     if (!(s = upload_plan(*full_[p])).ok()) return s;
@@ -438,10 +468,42 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       for (size_t k = i; k < j; k++) plan.h_lanes.push_back(folds[b][k]);
       plan.h_groups.push_back(G);
     }
+  // Terminal tasks: one warp per fold group; per showdown group, the
+  // ascending and descending passes and, when a terminal has a paired fold,
+  // the paired fold's pass. Launches ("waves") are bounded in tasks and in
+  // showdown groups (scratch).
+  plan.h_tasks.clear();
+  plan.waves.clear();
+  Plan::Wave wave;
+  auto close_wave = [&]() {
+    if (wave.count) plan.waves.push_back(wave);
+    wave = Plan::Wave();
+    wave.first = (uint32_t)plan.h_tasks.size();
+  };
+  wave.first = 0;
+  for (size_t gi = 0; gi < plan.h_groups.size(); gi++) {
+    const TermGroup& G = plan.h_groups[gi];
+    if (G.kind == T_FOLD_SCALAR || G.kind == T_FOLD_BATCH) {
+      if (wave.count + 1 > (uint32_t)MAX_WAVE_TASKS) close_wave();
+      plan.h_tasks.push_back(TermTask{R_FOLD, (uint32_t)gi, 0, 0});
+      wave.count += 1;
+      continue;
+    }
+    bool paired = false;
+    for (uint32_t k = 0; k < G.count; k++) paired |= plan.h_lanes[G.first + k].frow != NONE32;
+    const uint32_t need = paired ? 3 : 2;
+    if (wave.count + need > (uint32_t)MAX_WAVE_TASKS || wave.groups + 1 > (uint32_t)MAX_WAVE_GROUPS) close_wave();
+    const uint32_t wg = wave.groups++;
+    plan.h_tasks.push_back(TermTask{R_ASC, (uint32_t)gi, wg, 0});
+    plan.h_tasks.push_back(TermTask{R_DESC, (uint32_t)gi, wg, 0});
+    if (paired) plan.h_tasks.push_back(TermTask{R_PAIRED, (uint32_t)gi, wg, 0});
+    wave.count += need;
+  }
+  close_wave();
   int kernels = 0;
   for (auto& l : plan.down) kernels += l.count > 0;
   for (auto& l : plan.up) kernels += l.count > 0;
-  kernels += plan.h_groups.empty() ? 0 : 1;
+  kernels += (int)plan.waves.size();
   plan.kernels = kernels;
   return Status();
 }
@@ -452,6 +514,9 @@ Status Engine::upload_plan(Plan& plan) {
   if (!(s = dalloc(plan.d_up, plan.h_up.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_groups, plan.h_groups.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_lanes, plan.h_lanes.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_tasks, plan.h_tasks.size(), "plan")).ok()) return s;
+  if (!plan.h_tasks.empty())
+    CK(cudaMemcpy(plan.d_tasks, plan.h_tasks.data(), plan.h_tasks.size() * sizeof(TermTask), cudaMemcpyHostToDevice));
   if (!plan.h_down.empty())
     CK(cudaMemcpy(plan.d_down, plan.h_down.data(), plan.h_down.size() * sizeof(DownTask), cudaMemcpyHostToDevice));
   if (!plan.h_up.empty())
@@ -488,9 +553,20 @@ void Engine::term_args(int p, TermArgs& A) const {
   A.reach = reach_;
   A.vals = vals_;
   A.alive = alive_;
-  A.scratch = scratch_;
+  A.warp_scratch = warp_scratch_;
+  A.warp_scratch_floats = warp_scratch_floats_;
+  A.group_scratch = group_scratch_;
+  A.counters = counters_;
   A.tables = tables_;
   A.table_count = table_count_;
+  A.progs = progs_;
+  A.prog_count = prog_count_;
+  A.posmap = posmap_;
+  for (int q = 0; q < 2; q++) {
+    A.fold_prog[q] = fold_prog_[q];
+    A.emit_rec[q] = emit_rec_[q];
+  }
+  A.pstride = pstride_;
   for (int q = 0; q < 2; q++) {
     A.hc1[q] = hc1_[q];
     A.hc2[q] = hc2_[q];
@@ -517,12 +593,11 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   const int uchunks = (hp_[p] + ROW_CHUNK - 1) / ROW_CHUNK;
   for (const Plan::Level& l : plan.down)
     if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, dchunks, stream_);
-  if (!plan.h_groups.empty()) {
+  if (!plan.waves.empty()) {
     TermArgs T;
     term_args(p, T);
-    int ng = (int)plan.h_groups.size();
-    int blocks = std::min(term_blocks_, (ng + TERM_WARPS - 1) / TERM_WARPS);
-    launch_terminal(T, plan.d_groups, plan.d_lanes, ng, blocks, stream_);
+    for (const Plan::Wave& w : plan.waves)
+      launch_terminal(T, plan.d_groups, plan.d_lanes, plan.d_tasks + w.first, (int)w.count, stream_);
   }
   for (size_t d = plan.up.size(); d-- > 0;) {
     const Plan::Level& l = plan.up[d];
@@ -853,6 +928,12 @@ Status Engine::subtree_values(uint32_t root, int p, const std::vector<float>& op
   Plan plan;
   Status s;
   if (!(s = build_plan(root, p, plan)).ok()) return s;
+  for (const Plan::Wave& w : plan.waves)
+    if ((int)w.count > wave_tasks_ || (int)w.groups > wave_groups_) {
+      s.code = DCFR_ERR_INVALID_ARG;
+      s.msg = "subtree plan exceeds the terminal scratch";
+      return s;
+    }
   if (plan.nslots > max_slots_) {
     s.code = DCFR_ERR_INVALID_ARG;
     s.msg = "subtree plan exceeds the reach buffer";

@@ -20,10 +20,14 @@ struct TermArgs;
 // Kernel launchers (kernels.cu).
 void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s);
 void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s);
-void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, int ngroups, int blocks,
-                     cudaStream_t s);
+void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, const TermTask* tasks,
+                     int ntasks, cudaStream_t s);
 cudaError_t terminal_kernel_setup();
 size_t terminal_smem_bytes();
+void launch_programs(const EntryD* tables, const uint32_t* count, int tstride, uint32_t* progs, uint32_t* prog_count,
+                     uint32_t* posmap, int pstride, int nboards, cudaStream_t s);
+void launch_hand_program(const uint8_t* c1, const uint8_t* c2, const uint32_t* same, int n, int npad,
+                         uint32_t* fold_prog, uint2* emit_rec, cudaStream_t s);
 void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,
                      const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1, EntryD* out, uint32_t* count,
                      int tstride, cudaStream_t s);
@@ -52,6 +56,12 @@ struct Plan {
   std::vector<UpTask> h_up;
   std::vector<TermGroup> h_groups;
   std::vector<TermLane> h_lanes;
+  std::vector<TermTask> h_tasks;
+  struct Wave {
+    uint32_t first = 0, count = 0, groups = 0;
+  };
+  std::vector<Wave> waves;
+  TermTask* d_tasks = nullptr;
   DownTask* d_down = nullptr;
   UpTask* d_up = nullptr;
   TermGroup* d_groups = nullptr;
@@ -114,8 +124,17 @@ class Engine {
   EntryD* tables_ = nullptr;
   uint32_t* table_count_ = nullptr;
   int tstride_ = 0;
-  double* scratch_ = nullptr;
-  int term_blocks_ = 0;
+  uint32_t* progs_ = nullptr;
+  uint32_t* prog_count_ = nullptr;
+  uint32_t* posmap_ = nullptr;
+  uint32_t* fold_prog_[2] = {nullptr, nullptr};
+  uint2* emit_rec_[2] = {nullptr, nullptr};
+  int pstride_ = 0;
+  float* warp_scratch_ = nullptr;
+  size_t warp_scratch_floats_ = 0;
+  double* group_scratch_ = nullptr;
+  uint32_t* counters_ = nullptr;
+  int wave_tasks_ = 0, wave_groups_ = 0;
   DiscountD* disc_table_ = nullptr;
   uint32_t disc_len_ = 0;
   DiscountD* cur_disc_ = nullptr;

@@ -8,11 +8,7 @@
 //     128-bit loads and stores; all their arithmetic is per hand;
 //   * chance sums accumulate children in f64 in card order, then the
 //     isomorphic cards through the suit permutation (cfr.rs:462-478);
-//   * terminal values (terminal_kernel) run the reference's sequential
-//     strength-ordered sweeps (eval.rs:69-148, 214-344) in lockstep across the
-//     32 lanes of a warp, one terminal per lane, all lanes on the same board:
-//     the per-lane card-blocker sums live in shared memory ([52][32] f64), so
-//     every f64 sum is accumulated in the CPU's order.
+//   * terminal values are in terminal.cu.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -274,223 +270,6 @@ __global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask
   st4(A.vals + (size_t)T.node * stride + h0, out);
 }
 
-// ---------------------------------------------------------------- terminals
-__device__ __forceinline__ EntryD ld_entry(const EntryD* e) {
-  uint2 v = __ldg(reinterpret_cast<const uint2*>(e));
-  EntryD r;
-  r.strength = v.x;
-  r.idx = (uint16_t)(v.y & 0xFFFFu);
-  r.c1 = (uint8_t)((v.y >> 16) & 0xFFu);
-  r.c2 = (uint8_t)(v.y >> 24);
-  return r;
-}
-
-// Fold values for up to 32 fold terminals (one per lane): eval_fold
-// (eval.rs:40-64, kind T_FOLD_SCALAR) or fold_batch (eval.rs:173-206,
-// T_FOLD_BATCH); opponent sums in hand order.
-__device__ void fold_lanes(const TermArgs& A, uint32_t kind, bool live, const float* rr, float* orow, double pay,
-                           double (*mi)[32], int lane) {
-  const int p = A.p, o = p ^ 1;
-  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
-  double total = 0.0;
-  const uint8_t* oc1 = A.hc1[o];
-  const uint8_t* oc2 = A.hc2[o];
-  const int no = A.n[o];
-  for (int j = 0; j < no; j++) {
-    double w = live ? (double)rr[j] : 0.0;
-    total += w;
-    int a = __ldg(oc1 + j), b = __ldg(oc2 + j);
-    mi[a][lane] += w;
-    mi[b][lane] += w;
-  }
-  const int np = A.n[p], hp = A.hp[p];
-  const uint8_t* pc1 = A.hc1[p];
-  const uint8_t* pc2 = A.hc2[p];
-  const uint32_t* same = A.same[p];
-  for (int h = 0; h < hp; h++) {
-    float f = 0.0f;
-    if (h < np) {
-      double a = mi[__ldg(pc1 + h)][lane], b = mi[__ldg(pc2 + h)][lane];
-      uint32_t sm = __ldg(same + h);
-      double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
-      if (kind == T_FOLD_SCALAR)
-        f = total == 0.0 ? 0.0f : (float)(pay * ((total - (a + b)) + sw));
-      else
-        f = (float)(pay * (((total - a) - b) + sw));
-    }
-    if (live) orow[h] = f;
-  }
-}
-
-// Showdown values for up to 32 showdown terminals on one board: eval_showdown
-// (eval.rs:69-148, T_SHOWDOWN_SCALAR) or showdown_batch (eval.rs:214-344,
-// T_SHOWDOWN_BATCH, with the paired fold read off the ascending sweep).
-__device__ void showdown_lanes(const TermArgs& A, const TermGroup& G, const TermLane& L, bool live, const float* rr,
-                               float* orow, double (*mi)[32], double* scr, int lane) {
-  const int p = A.p, o = p ^ 1;
-  const EntryD* mine = A.tables + (size_t)(G.board * 2 + p) * A.tstride;
-  const EntryD* theirs = A.tables + (size_t)(G.board * 2 + o) * A.tstride;
-  const int cm = (int)A.table_count[G.board * 2 + p];
-  const int ct = (int)A.table_count[G.board * 2 + o];
-  const bool batch = G.kind == T_SHOWDOWN_BATCH;
-  const int hp = A.hp[p];
-  // Zero the rows of live lanes (hands blocked by the board stay 0).
-  unsigned lm = __ballot_sync(0xffffffffu, live);
-  while (lm) {
-    int t = __ffs(lm) - 1;
-    lm &= lm - 1;
-    uint32_t row = __shfl_sync(0xffffffffu, L.row, t);
-    float* r = A.vals + (size_t)row * A.stride;
-    for (int h = lane * VEC; h < hp; h += 32 * VEC) st4(r + h, make_float4(0.f, 0.f, 0.f, 0.f));
-  }
-  __syncwarp();
-  // Pass 1, ascending: opponent hands strictly weaker.
-  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
-  double sum = 0.0;
-  int i = 0, j = 0;
-  while (i < cm) {
-    const uint32_t s = ld_entry(mine + i).strength;
-    while (j < ct) {
-      EntryD e = ld_entry(theirs + j);
-      if (e.strength >= s) break;
-      double w = live ? (double)rr[e.idx] : 0.0;
-      sum += w;
-      mi[e.c1][lane] += w;
-      mi[e.c2][lane] += w;
-      j++;
-    }
-    while (i < cm) {
-      EntryD e = ld_entry(mine + i);
-      if (e.strength != s) break;
-      double a = mi[e.c1][lane], b = mi[e.c2][lane];
-      scr[(size_t)i * 32 + lane] = batch ? L.a * ((sum - a) - b) : L.a * (sum - (a + b));
-      i++;
-    }
-  }
-  // Paired fold: finish the sweep and read the fold off the sums.
-  const bool has_fold = batch && live && L.frow != NONE32;
-  if (__any_sync(0xffffffffu, has_fold)) {
-    while (j < ct) {
-      EntryD e = ld_entry(theirs + j);
-      double w = live ? (double)rr[e.idx] : 0.0;
-      sum += w;
-      mi[e.c1][lane] += w;
-      mi[e.c2][lane] += w;
-      j++;
-    }
-    float* frow = A.vals + (size_t)(has_fold ? L.frow : 0) * A.stride;
-    const int np = A.n[p];
-    for (int h = 0; h < hp; h++) {
-      float f = 0.0f;
-      if (h < np) {
-        double a = mi[__ldg(A.hc1[p] + h)][lane], b = mi[__ldg(A.hc2[p] + h)][lane];
-        uint32_t sm = __ldg(A.same[p] + h);
-        double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
-        f = (float)(L.d * (((sum - a) - b) + sw));
-      }
-      if (has_fold) frow[h] = f;
-    }
-  }
-  // Pass 2, descending: opponent hands strictly stronger.
-  for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
-  sum = 0.0;
-  i = cm;
-  j = ct;
-  while (i > 0) {
-    const uint32_t s = ld_entry(mine + i - 1).strength;
-    while (j > 0) {
-      EntryD e = ld_entry(theirs + j - 1);
-      if (e.strength <= s) break;
-      double w = live ? (double)rr[e.idx] : 0.0;
-      sum += w;
-      mi[e.c1][lane] += w;
-      mi[e.c2][lane] += w;
-      j--;
-    }
-    while (i > 0) {
-      EntryD e = ld_entry(mine + i - 1);
-      if (e.strength != s) break;
-      double a = mi[e.c1][lane], b = mi[e.c2][lane];
-      double W = scr[(size_t)(i - 1) * 32 + lane];
-      float v;
-      if (batch)
-        v = (float)(W + L.b * ((sum - a) - b));
-      else
-        v = (float)W + (float)(L.b * (sum - (a + b)));
-      if (live) orow[e.idx] = v;
-      i--;
-    }
-  }
-  // Ties (add_ties, eval.rs:347-379) when the tie payoff is nonzero.
-  const bool tie = live && L.c != 0.0;
-  if (__any_sync(0xffffffffu, tie)) {
-    for (int c = 0; c < 52; c++) mi[c][lane] = 0.0;
-    int k = 0;
-    j = 0;
-    while (k < cm) {
-      const uint32_t s = ld_entry(mine + k).strength;
-      while (j < ct && ld_entry(theirs + j).strength < s) j++;
-      double eq_sum = 0.0;
-      int jj = j;
-      while (jj < ct) {
-        EntryD e = ld_entry(theirs + jj);
-        if (e.strength != s) break;
-        double w = live ? (double)rr[e.idx] : 0.0;
-        eq_sum += w;
-        mi[e.c1][lane] += w;
-        mi[e.c2][lane] += w;
-        jj++;
-      }
-      while (k < cm) {
-        EntryD e = ld_entry(mine + k);
-        if (e.strength != s) break;
-        uint32_t sm = __ldg(A.same[p] + e.idx);
-        double sw = (sm != NONE32 && live) ? (double)rr[sm] : 0.0;
-        double eq = (eq_sum - (mi[e.c1][lane] + mi[e.c2][lane])) + sw;
-        if (tie) orow[e.idx] += (float)(L.c * eq);
-        k++;
-      }
-      for (int q = j; q < jj; q++) {
-        EntryD e = ld_entry(theirs + q);
-        mi[e.c1][lane] = 0.0;
-        mi[e.c2][lane] = 0.0;
-      }
-    }
-  }
-}
-
-__global__ void __launch_bounds__(TERM_WARPS * 32) terminal_kernel(TermArgs A, const TermGroup* __restrict__ groups,
-                                                                    const TermLane* __restrict__ lanes, int ngroups) {
-  extern __shared__ double smem_minus[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double(*mi)[32] = reinterpret_cast<double(*)[32]>(smem_minus + (size_t)warp * 52 * 32);
-  const int gw = blockIdx.x * TERM_WARPS + warp;
-  const int nw = gridDim.x * TERM_WARPS;
-  double* scr = A.scratch + (size_t)gw * A.nmax * 32;
-  for (int g = gw; g < ngroups; g += nw) {
-    const TermGroup G = groups[g];
-    const bool act = lane < (int)G.count;
-    TermLane L;
-    if (act) {
-      L = lanes[G.first + lane];
-    } else {
-      L.slot = 0;
-      L.row = 0;
-      L.frow = NONE32;
-      L.pad = 0;
-      L.a = L.b = L.c = L.d = 0.0;
-    }
-    const bool live = act && A.alive[L.slot] != 0;
-    const float* rr = A.reach + (size_t)L.slot * A.stride;
-    float* orow = A.vals + (size_t)L.row * A.stride;
-    if (G.kind == T_FOLD_SCALAR || G.kind == T_FOLD_BATCH)
-      fold_lanes(A, G.kind, live, rr, orow, L.a, mi, lane);
-    else
-      showdown_lanes(A, G, L, live, rr, orow, mi, scr, lane);
-    __syncwarp();
-  }
-}
-
 // ------------------------------------------------------------ setup kernels
 // 7-card strength (crates/holdem/src/eval.rs:104-198): category<<26 | payload.
 __device__ __forceinline__ uint32_t hb(uint32_t x) { return 31u - (uint32_t)__clz(x); }
@@ -703,17 +482,6 @@ void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int nt
     else if (mode == M_BR) launch_up_t<M_BR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
     else launch_up_t<M_AVG, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
   }
-}
-
-size_t terminal_smem_bytes() { return (size_t)TERM_WARPS * 52 * 32 * sizeof(double); }
-
-cudaError_t terminal_kernel_setup() {
-  return cudaFuncSetAttribute(terminal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)terminal_smem_bytes());
-}
-
-void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, int ngroups, int blocks,
-                     cudaStream_t s) {
-  terminal_kernel<<<blocks, TERM_WARPS * 32, terminal_smem_bytes(), s>>>(A, groups, lanes, ngroups);
 }
 
 void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,

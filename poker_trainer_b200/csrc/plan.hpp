@@ -23,6 +23,7 @@ constexpr int ROW_THREADS = 128;   // threads per row-kernel block
 constexpr int ROW_CHUNK = VEC * ROW_THREADS;
 constexpr int MAX_ACTIONS = 16;
 constexpr int TERM_WARPS = 4;      // warps per terminal-kernel block
+constexpr int TERM_CHUNK = 32;     // sweep steps staged per cp.async batch
 constexpr uint32_t NONE32 = 0xFFFFFFFFu;
 
 enum DownKind : uint32_t { D_OPP_SPLIT = 0, D_CHANCE_SPLIT = 1 };
@@ -71,6 +72,19 @@ struct TermLane {
   double d;       // paired fold payoff
 };
 
+// One warp's work in the terminal kernel: a fold group, or one of the
+// passes of a showdown group (ascending win part, descending lose part,
+// paired fold). wgroup indexes the per-launch win/lose scratch and counter.
+enum TermRole : uint32_t { R_FOLD = 0, R_ASC = 1, R_DESC = 2, R_PAIRED = 3 };
+struct TermTask {
+  uint32_t role;
+  uint32_t group;
+  uint32_t wgroup;
+  uint32_t pad;
+};
+constexpr int MAX_WAVE_TASKS = 1024;   // warps per terminal launch
+constexpr int MAX_WAVE_GROUPS = 384;   // showdown groups per terminal launch
+
 struct TermGroup {
   uint32_t kind;
   uint32_t board;  // showdown strength table
@@ -114,9 +128,18 @@ struct TermArgs {
   const float* reach;
   float* vals;
   const uint32_t* alive;
-  double* scratch;  // [warps][nmax][32]
+  float* warp_scratch;          // per warp: Rp [pstride+1][32], O [stride][32]
+  size_t warp_scratch_floats;
+  double* group_scratch;        // per showdown group: win and lose parts [2][nmax][32]
+  uint32_t* counters;           // per showdown group: passes finished
   const EntryD* tables;
   const uint32_t* table_count;
+  const uint32_t* progs;        // [((board*2+p)*3+dir)][pstride] sweep programs
+  const uint32_t* prog_count;   // steps per program (a multiple of TERM_CHUNK)
+  const uint32_t* posmap;       // [((board*2+p)*3+dir)][tstride] opponent hand -> step
+  const uint32_t* fold_prog[2]; // each player's hands in hand order as steps
+  const uint2* emit_rec[2];     // per hand: blocker rows word, identical opponent hand
+  int pstride;
   const uint8_t* hc1[2];
   const uint8_t* hc2[2];
   const uint32_t* same[2];
