@@ -57,6 +57,13 @@ enum { DCFR_FOLD = 0, DCFR_CHECK = 1, DCFR_CALL = 2, DCFR_RAISE = 3 };
 /* Storage modes (StorageMode, crates/solver/src/storage.rs:79-85). */
 enum { DCFR_STORAGE_F32 = 0, DCFR_STORAGE_COMPRESSED = 1, DCFR_STORAGE_AUTO = 2 };
 
+/* GpuPrecision (crates/solver/src/gpu/mod.rs:51-63). FAST (the default, as
+ * in the reference) evaluates terminals with exact 64-bit fixed-point sums of
+ * the f32 reach, which agree with the CPU's sequential f64 sums except for
+ * rare one-rounding-step differences; EXACT sweeps in the CPU's f64
+ * operation order and is bit-identical to the CPU solver. */
+enum { DCFR_PRECISION_FAST = 0, DCFR_PRECISION_EXACT = 1 };
+
 /* Traversal modes (cfr::Mode, crates/solver/src/cfr.rs:248-256). */
 enum { DCFR_MODE_CFR = 0, DCFR_MODE_BEST_RESPONSE = 1, DCFR_MODE_AVERAGE = 2 };
 
@@ -140,6 +147,8 @@ typedef struct dcfr_config {
   int32_t storage;
   int32_t isomorphism;
   dcfr_params dcfr;
+  int32_t precision; /* DCFR_PRECISION_* (Solver::use_gpu(precision), lib.rs:508-530) */
+  int32_t _pad4;
 } dcfr_config;
 
 /* TreeStats (crates/solver/src/tree.rs:248-257). */

@@ -29,6 +29,8 @@ PREFLOP, FLOP, TURN, RIVER = 0, 1, 2, 3
 SIZE_POT, SIZE_MULT, SIZE_ALLIN = 0, 1, 2
 FOLD, CHECK, CALL, RAISE = 0, 1, 2, 3
 STORAGE_F32, STORAGE_COMPRESSED, STORAGE_AUTO = 0, 1, 2
+PRECISION_FAST, PRECISION_EXACT = 0, 1  # GpuPrecision (crates/solver/src/gpu/mod.rs:51-63)
+PRECISIONS = {"fast": PRECISION_FAST, "exact": PRECISION_EXACT}
 MODE_CFR, MODE_BEST_RESPONSE, MODE_AVERAGE = 0, 1, 2
 
 
@@ -108,6 +110,8 @@ class Config(C.Structure):
         ("storage", C.c_int32),
         ("isomorphism", C.c_int32),
         ("dcfr", Params),
+        ("precision", C.c_int32),
+        ("_pad4", C.c_int32),
     ]
 
 
@@ -294,7 +298,7 @@ def make_config(board, ranges, *, root=None, pot=None, stack=None, menu_: Menu |
                 future_menu: Menu | None = None, big_blind=100, prune=0.0, keep=((), ()),
                 max_memory_bytes=8 << 30, rake_rate=0.0, rake_cap=0.0, storage=STORAGE_AUTO,
                 isomorphism=True, alpha=1.5, beta=0.0, beta_clip=False, gamma=3.0,
-                restart_average=True, unweighted_average=True) -> Config:
+                restart_average=True, unweighted_average=True, precision="fast") -> Config:
     """SolveConfig (crates/solver/src/lib.rs:74-135), defaults as
     SolveConfig::new and DcfrParams::default (cfr.rs:72-80)."""
     cfg = Config()
@@ -329,6 +333,7 @@ def make_config(board, ranges, *, root=None, pot=None, stack=None, menu_: Menu |
     cfg.dcfr.alpha, cfg.dcfr.beta, cfg.dcfr.gamma = alpha, beta, gamma
     cfg.dcfr.beta_clip = int(beta_clip)
     cfg.dcfr.restart_average, cfg.dcfr.unweighted_average = int(restart_average), int(unweighted_average)
+    cfg.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     return cfg
 
 

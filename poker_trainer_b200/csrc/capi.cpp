@@ -71,6 +71,7 @@ int dcfr_config_init(dcfr_config* cfg) {
   cfg->dcfr.gamma = 3.0;
   cfg->dcfr.restart_average = 1;
   cfg->dcfr.unweighted_average = 1;
+  cfg->precision = DCFR_PRECISION_FAST;
   return DCFR_OK;
 }
 

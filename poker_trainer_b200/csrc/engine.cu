@@ -52,6 +52,7 @@ Plan::~Plan() {
   dfree(d_groups);
   dfree(d_lanes);
   dfree(d_tasks);
+  dfree(d_fast);
 }
 
 // DcfrParams -> Discount (cfr.rs:86-106), host f64 pow as the reference.
@@ -96,6 +97,12 @@ static uint32_t next_gap(bool has_prev, uint32_t t0, double e0, uint32_t t, doub
 Status Engine::create(const dcfr_config& cfg, std::unique_ptr<Engine>& out) {
   std::unique_ptr<Engine> e(new Engine());
   Status s;
+  if (cfg.precision != DCFR_PRECISION_FAST && cfg.precision != DCFR_PRECISION_EXACT) {
+    s.code = DCFR_ERR_INVALID_ARG;
+    s.msg = "precision must be DCFR_PRECISION_FAST or DCFR_PRECISION_EXACT";
+    return s;
+  }
+  e->fast_ = cfg.precision == DCFR_PRECISION_FAST;
   s.code = build_game(cfg, e->g, s.msg, true);
   if (!s.ok()) return s;
   s = e->init();
@@ -136,6 +143,9 @@ Engine::~Engine() {
   dfree(warp_scratch_);
   dfree(group_scratch_);
   dfree(counters_);
+  dfree(fcat_);
+  dfree(fseg_);
+  dfree(frec_);
   dfree(disc_table_);
   dfree(cur_disc_);
   dfree(counter_);
@@ -214,6 +224,7 @@ Status Engine::init() {
     CK(cudaMemcpy(hc1_[q], a.data(), hp_[q], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(hc2_[q], b.data(), hp_[q], cudaMemcpyHostToDevice));
     CK(cudaMemcpy(same_[q], sm.data(), hp_[q] * 4, cudaMemcpyHostToDevice));
+    if (fast_) continue;
     // The player's hands in hand order as sweep steps (fold sums) and per-hand
     // emit records (terminal.cu).
     const int npad = (g.n[q] + TERM_CHUNK - 1) / TERM_CHUNK * TERM_CHUNK;
@@ -265,14 +276,33 @@ Status Engine::init() {
       launch_strength(d_boards, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1], tables_, table_count_,
                       tstride_, stream_);
       CK(cudaGetLastError());
-      // Sweep programs (terminal.cu): per board, traverser and pass.
-      if (!(s = dalloc(progs_, (size_t)nb * 6 * pstride_, "sweep programs")).ok()) return s;
-      if (!(s = dalloc(prog_count_, (size_t)nb * 6, "sweep programs")).ok()) return s;
-      if (!(s = dalloc(posmap_, (size_t)nb * 6 * tstride_, "sweep programs")).ok()) return s;
-      launch_programs(tables_, table_count_, tstride_, progs_, prog_count_, posmap_, pstride_, nb, stream_);
-      CK(cudaGetLastError());
+      if (!fast_) {
+        // Sweep programs (terminal.cu): per board, traverser and pass.
+        if (!(s = dalloc(progs_, (size_t)nb * 6 * pstride_, "sweep programs")).ok()) return s;
+        if (!(s = dalloc(prog_count_, (size_t)nb * 6, "sweep programs")).ok()) return s;
+        if (!(s = dalloc(posmap_, (size_t)nb * 6 * tstride_, "sweep programs")).ok()) return s;
+        launch_programs(tables_, table_count_, tstride_, progs_, prog_count_, posmap_, pstride_, nb, stream_);
+        CK(cudaGetLastError());
+      }
       CK(cudaStreamSynchronize(stream_));
       cudaFree(d_boards);
+    }
+    if (fast_) {
+      // Scan layouts (terminal_fast.cu): the boards' tables, then the fold layout.
+      fcstride_ = (3 * tstride_ + 7) / 8 * 8;
+      femax_ = fast_emax(tstride_);
+      const size_t nl = (size_t)(nb + 1) * 2;
+      if (!(s = dalloc(fcat_, nl * fcstride_, "scan layouts")).ok()) return s;
+      if (!(s = dalloc(fseg_, nl * FAST_SEGS, "scan layouts")).ok()) return s;
+      if (!(s = dalloc(frec_, nl * tstride_, "scan layouts")).ok()) return s;
+      launch_fast_layouts(tables_, table_count_, tstride_, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1],
+                          fcat_, fseg_, frec_, fcstride_, stream_);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(stream_));
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      fast_blocks_ = sms * fast_blocks_per_sm(stride_, femax_);
     }
   }
   // Plans for the two traversals of an iteration.
@@ -296,7 +326,7 @@ Status Engine::init() {
     if (!(s = dalloc(root_out_, rr.size(), "root rows")).ok()) return s;
   }
   // Terminal scratch, sized for the largest terminal launch of the two plans.
-  {
+  if (!fast_) {
     for (int p = 0; p < 2; p++)
       for (const Plan::Wave& w : full_[p]->waves) {
         wave_tasks_ = std::max<int>(wave_tasks_, (int)w.count);
@@ -468,6 +498,16 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       for (size_t k = i; k < j; k++) plan.h_lanes.push_back(folds[b][k]);
       plan.h_groups.push_back(G);
     }
+  // Fast precision: one task per terminal, showdowns by board, then folds.
+  plan.h_fast.clear();
+  for (const SdLane& x : sd) {
+    const TermLane& L = x.lane;
+    plan.h_fast.push_back(FastTask{x.kind, x.board, L.slot, L.row, L.frow, {0, 0, 0}, L.a, L.b, L.c, L.d});
+  }
+  for (int b = 0; b < 2; b++)
+    for (const TermLane& L : folds[b])
+      plan.h_fast.push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, (uint32_t)g.boards.size(),
+                                     L.slot, L.row, NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
   // Terminal tasks: one warp per fold group; per showdown group, the
   // ascending and descending passes and, when a terminal has a paired fold,
   // the paired fold's pass. Launches ("waves") are bounded in tasks and in
@@ -503,7 +543,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   int kernels = 0;
   for (auto& l : plan.down) kernels += l.count > 0;
   for (auto& l : plan.up) kernels += l.count > 0;
-  kernels += (int)plan.waves.size();
+  kernels += fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
   plan.kernels = kernels;
   return Status();
 }
@@ -515,6 +555,9 @@ Status Engine::upload_plan(Plan& plan) {
   if (!(s = dalloc(plan.d_groups, plan.h_groups.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_lanes, plan.h_lanes.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_tasks, plan.h_tasks.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_fast, plan.h_fast.size(), "plan")).ok()) return s;
+  if (!plan.h_fast.empty())
+    CK(cudaMemcpy(plan.d_fast, plan.h_fast.data(), plan.h_fast.size() * sizeof(FastTask), cudaMemcpyHostToDevice));
   if (!plan.h_tasks.empty())
     CK(cudaMemcpy(plan.d_tasks, plan.h_tasks.data(), plan.h_tasks.size() * sizeof(TermTask), cudaMemcpyHostToDevice));
   if (!plan.h_down.empty())
@@ -580,6 +623,25 @@ void Engine::term_args(int p, TermArgs& A) const {
   A.p = p;
 }
 
+void Engine::fast_args(int p, FastArgs& A) const {
+  A.reach = reach_;
+  A.vals = vals_;
+  A.alive = alive_;
+  A.cat = fcat_;
+  A.seg = fseg_;
+  A.rec = frec_;
+  A.same = same_[p];
+  A.cstride = fcstride_;
+  A.tstride = tstride_;
+  A.emax = femax_;
+  for (int q = 0; q < 2; q++) {
+    A.n[q] = g.n[q];
+    A.hp[q] = hp_[q];
+  }
+  A.stride = stride_;
+  A.p = p;
+}
+
 // Enqueues one traversal: liveness reset, root row, down levels, terminals,
 // up levels (deepest first); the root's value row is copied to root_out.
 void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out) {
@@ -593,7 +655,13 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   const int uchunks = (hp_[p] + ROW_CHUNK - 1) / ROW_CHUNK;
   for (const Plan::Level& l : plan.down)
     if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, dchunks, stream_);
-  if (!plan.waves.empty()) {
+  if (fast_) {
+    if (!plan.h_fast.empty()) {
+      FastArgs F;
+      fast_args(p, F);
+      launch_fast_terminal(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, stream_);
+    }
+  } else if (!plan.waves.empty()) {
     TermArgs T;
     term_args(p, T);
     for (const Plan::Wave& w : plan.waves)
@@ -929,7 +997,7 @@ Status Engine::subtree_values(uint32_t root, int p, const std::vector<float>& op
   Status s;
   if (!(s = build_plan(root, p, plan)).ok()) return s;
   for (const Plan::Wave& w : plan.waves)
-    if ((int)w.count > wave_tasks_ || (int)w.groups > wave_groups_) {
+    if (!fast_ && ((int)w.count > wave_tasks_ || (int)w.groups > wave_groups_)) {
       s.code = DCFR_ERR_INVALID_ARG;
       s.msg = "subtree plan exceeds the terminal scratch";
       return s;

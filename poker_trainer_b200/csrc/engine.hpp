@@ -31,6 +31,12 @@ void launch_hand_program(const uint8_t* c1, const uint8_t* c2, const uint32_t* s
 void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,
                      const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1, EntryD* out, uint32_t* count,
                      int tstride, cudaStream_t s);
+void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstride, int nboards, const uint8_t* hc1_0,
+                         const uint8_t* hc2_0, const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1,
+                         uint16_t* cat, uint16_t* seg, uint4* rec, int cstride, cudaStream_t s);
+void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
+int fast_emax(int tstride);
+int fast_blocks_per_sm(int stride, int emax);
 void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
 void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
 void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
@@ -57,6 +63,7 @@ struct Plan {
   std::vector<TermGroup> h_groups;
   std::vector<TermLane> h_lanes;
   std::vector<TermTask> h_tasks;
+  std::vector<FastTask> h_fast;  // fast precision: one task per terminal
   struct Wave {
     uint32_t first = 0, count = 0, groups = 0;
   };
@@ -66,6 +73,7 @@ struct Plan {
   UpTask* d_up = nullptr;
   TermGroup* d_groups = nullptr;
   TermLane* d_lanes = nullptr;
+  FastTask* d_fast = nullptr;
   int kernels = 0;  // kernel launches per traversal
   uint64_t nodes = 0;
   ~Plan();
@@ -135,6 +143,12 @@ class Engine {
   double* group_scratch_ = nullptr;
   uint32_t* counters_ = nullptr;
   int wave_tasks_ = 0, wave_groups_ = 0;
+  // Fast precision (terminal_fast.cu): scan layouts per (layout, traverser).
+  bool fast_ = true;
+  uint16_t* fcat_ = nullptr;
+  uint16_t* fseg_ = nullptr;
+  uint4* frec_ = nullptr;
+  int fcstride_ = 0, femax_ = 0, fast_blocks_ = 0;
   DiscountD* disc_table_ = nullptr;
   uint32_t disc_len_ = 0;
   DiscountD* cur_disc_ = nullptr;
@@ -150,6 +164,7 @@ class Engine {
   Status upload_plan(Plan& plan);
   void row_args(int p, RowArgs& A) const;
   void term_args(int p, TermArgs& A) const;
+  void fast_args(int p, FastArgs& A) const;
   void enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out);
   Status ensure_discounts(uint32_t max_t);
   Status capture_graphs();

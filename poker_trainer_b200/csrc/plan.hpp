@@ -104,6 +104,45 @@ struct DiscountD {
   int reach_weighted;
 };
 
+// Fast-precision terminal evaluation (terminal_fast.cu): one task per live
+// terminal; a showdown task also writes its paired fold's row.
+struct FastTask {
+  uint32_t kind;   // TermKind
+  uint32_t board;  // layout index: showdown board, or the fold layout
+  uint32_t slot;   // reach slot
+  uint32_t row;    // value row (node id)
+  uint32_t frow;   // paired fold's value row, or NONE32
+  uint32_t pad[3];
+  double a, b, c, d;  // as TermLane
+};
+
+// Per (layout, traverser) scan layout of the opponent's hands: segment 0
+// lists them in ascending strength, segment 1+c lists those holding card c
+// (ascending strength). seg[j] is the first element of segment j
+// (seg[53] = 3 * count). Per traverser hand h, rec[h] = {w | s << 16,
+// aw | as << 16, bw | bs << 16, a | b << 8 | present << 16}: w (s) counts the
+// opponent hands weaker than (not stronger than) h, aw/as (bw/bs) index the
+// same boundaries inside card a's (b's) segment.
+constexpr int FAST_SEGS = 54;
+constexpr int FAST_THREADS = 256;
+
+struct FastArgs {
+  const float* reach;
+  float* vals;
+  const uint32_t* alive;
+  const uint16_t* cat;   // [(layout*2+p)][cstride] opponent hand per element
+  const uint16_t* seg;   // [(layout*2+p)][FAST_SEGS]
+  const uint4* rec;      // [(layout*2+p)][tstride]
+  const uint32_t* same;  // traverser hand -> identical opponent hand (or NONE32)
+  int cstride;
+  int tstride;
+  int emax;              // elements per thread (odd) for the largest layout
+  int n[2];
+  int hp[2];
+  int stride;
+  int p;
+};
+
 // Arguments of the row kernels (down/up levels) of one traversal.
 struct RowArgs {
   float* regrets;

@@ -1,0 +1,167 @@
+"""Fast precision (the default, GpuPrecision::Fast,
+crates/solver/src/gpu/mod.rs:53-58) against the CPU oracle, by the standards of
+the reference's own fast-mode GPU tests (crates/solver/src/gpu/engine/tests.rs):
+
+- traversal values within 1e-5 of the row's scale
+  (random_turn_spots_match_cpu_fast, tests.rs:514-540);
+- 5-iteration solves within 5e-5 in strategy and 0.25 chips in EV
+  (fast_short_solves_match_cpu, tests.rs:481-490);
+- converged solves reach the target in a similar number of iterations with
+  range-level strategies within 0.03 (fast_converged_solves_match_cpu,
+  tests.rs:492-512);
+- and, for the benchmark workloads, exploitability after the same iteration
+  count within 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+import spots
+from oracle_api import OracleSolver
+from poker_trainer_b200 import abi, workloads
+from poker_trainer_b200.solver import Solver, SolveOptions
+
+pytestmark = pytest.mark.gpu
+
+SPOTS = {
+    "river": (spots.river_config, []),
+    "turn": (spots.turn_config, ["Ks", "2h"]),
+    "iso_turn": (spots.iso_turn_config, ["Kc", "Kh", "3s"]),
+    "allin_turn": (spots.allin_turn_config, ["Ah"]),
+    "mid_street_raked": (lambda: spots.mid_street_config(True), []),
+    "mid_street": (lambda: spots.mid_street_config(False), []),
+}
+
+TRAVERSAL_TOL = 1e-5  # of the row's largest magnitude
+STRATEGY_TOL = 5e-5
+EV_TOL_CHIPS = 0.25
+EXPLOITABILITY_RTOL = 1e-4
+
+
+def diff_and_scale(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    assert a.shape == b.shape
+    return float(np.max(np.abs(a - b), initial=0.0)), float(np.max(np.abs(b), initial=0.0))
+
+
+def assert_relative(a, b, tol, what):
+    assert np.all(np.isfinite(a)), f"{what}: non-finite GPU value"
+    diff, scale = diff_and_scale(a, b)
+    assert diff <= tol * max(scale, 1e-30), f"{what}: max diff {diff:e} vs scale {scale:e}"
+
+
+def random_storage(n, seed):
+    rng = np.random.default_rng(seed)
+    r = (rng.standard_normal(n) * 50).astype(np.float32)
+    r[rng.random(n) < 0.3] = 0.0
+    s = (rng.random(n) * 10).astype(np.float32)
+    s[rng.random(n) < 0.2] = 0.0
+    return r, s
+
+
+def compare_nodes(o, g, strat_tol, ev_tol, rivers):
+    paths = [[], ["check"], ["fold"]] + [["check", "check", c] for c in rivers]
+    for path in paths:
+        try:
+            qo = o.query(path)
+        except Exception:
+            assert len(path) <= 2, f"river path {path} not found"
+            continue
+        qg = g.query(path)
+        assert qg.actions == qo["actions"], path
+        assert np.array_equal(qg.combos, qo["combos"]), path
+        ds, _ = diff_and_scale(qg.strategy.ravel(), qo["strategy"].ravel())
+        de, _ = diff_and_scale(qg.ev.ravel(), qo["ev"].ravel())
+        assert ds <= strat_tol, f"{path}: strategy differs by {ds:e}"
+        assert de <= ev_tol, f"{path}: EV differs by {de} chips"
+
+
+@pytest.mark.parametrize("name", list(SPOTS))
+def test_fast_traversal_values_match(gpu, name):
+    cfg = SPOTS[name][0]()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    r, s = random_storage(g.storage_len(), 11)
+    identical = total = 0
+    for p in (0, 1):
+        for mode in (abi.MODE_BEST_RESPONSE, abi.MODE_AVERAGE, abi.MODE_CFR):
+            o.set_storage(r, s)
+            g.upload_storage(r, s)
+            vo = np.asarray(o.traverse(p, mode, 5), np.float32)
+            vg = np.asarray(g.traverse(p, mode, 5), np.float32)
+            assert_relative(vg, vo, TRAVERSAL_TOL, f"{name} p={p} mode={mode}")
+            identical += int(np.sum(vg.view(np.uint32) == vo.view(np.uint32)))
+            total += vg.size
+            if mode == abi.MODE_CFR:
+                ro, so = o.storage()
+                rg, sg = g.download_storage()
+                assert_relative(rg, ro, TRAVERSAL_TOL, f"{name} p={p} regrets")
+                assert_relative(sg, so, TRAVERSAL_TOL, f"{name} p={p} sums")
+    # Root values sum many terminals; most still come out bit-identical.
+    assert identical >= 0.9 * total, f"{name}: only {identical} of {total} root values identical"
+
+
+@pytest.mark.parametrize("name", list(SPOTS))
+def test_fast_short_solves_match(gpu, name):
+    make, rivers = SPOTS[name]
+    cfg = make()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(5)
+    g.iterate(5)
+    compare_nodes(o, g, STRATEGY_TOL, EV_TOL_CHIPS, rivers)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_fast_random_turn_spots(gpu, seed):
+    cfg = spots.random_turn_config(seed)
+    try:
+        o = OracleSolver(cfg)
+    except Exception:
+        pytest.skip("spot rejected by Solver::new")
+    g = Solver.new(cfg)
+    r, s = random_storage(g.storage_len(), 100 + seed)
+    for p in (0, 1):
+        for mode in (abi.MODE_AVERAGE, abi.MODE_BEST_RESPONSE):
+            o.set_storage(r, s)
+            g.upload_storage(r, s)
+            assert_relative(g.traverse(p, mode, 1), o.traverse(p, mode, 1), TRAVERSAL_TOL, f"p={p} mode={mode}")
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(4)
+    g.iterate(4)
+    ev_scale = float(np.max(np.abs(o.query([])["ev"])))
+    compare_nodes(o, g, STRATEGY_TOL, EV_TOL_CHIPS * (1.0 + ev_scale / 2500.0), [])
+
+
+@pytest.mark.parametrize("name", ["turn", "iso_turn"])
+def test_fast_converged_solves(gpu, name):
+    cfg = SPOTS[name][0]()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    po = o.solve(400, 0.3, 20)
+    pg = g.solve(SolveOptions(max_iterations=400, target_exploitability_pct=0.3, check_every=20))
+    assert po.exploitability_pct <= 0.3 and pg.exploitability_pct <= 0.3, (po.exploitability_pct, pg)
+    ic, ig = po.iteration, pg.iteration
+    assert abs(ic - ig) <= 0.2 * ic, f"iterations to target: cpu {ic}, gpu {ig}"
+    for path in ([], ["check"]):
+        a = np.asarray(g.query(path).range_strategy())
+        qo = o.query(path)
+        w = qo["reach"].astype(np.float64)
+        b = (qo["strategy"].astype(np.float64) * w[None, :]).sum(axis=1) / max(w.sum(), 1e-30)
+        assert np.all(np.abs(a - b) < 0.03), (path, a, b)
+
+
+@pytest.mark.parametrize("spot", ["river", "turn"])
+def test_fast_workload_exploitability(gpu, spot):
+    """The benchmark workloads (river Ks7s2dTh4c and turn Ks7s2dTh, 1000
+    iterations, alpha 1.5 beta 0 gamma 2): exploitability within 1e-4
+    relative of the oracle's after the same iterations."""
+    cfg = workloads.river_spot() if spot == "river" else workloads.turn_spot()
+    iters = 1000 if spot == "river" else 200
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    o.iterate(iters)
+    g.iterate(iters)
+    eo, eg = o.exploitability(), g.exploitability()
+    assert abs(eg - eo) <= EXPLOITABILITY_RTOL * abs(eo), (eg, eo)

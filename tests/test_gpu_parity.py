@@ -1,6 +1,8 @@
 """GPU parity against the CPU oracle (the C++ restatement of the reference's
-CPU DCFR solver). The GPU path performs the reference's floating-point
-operations in the reference's order, so the bar is bit-identical results:
+CPU DCFR solver) in exact precision (GpuPrecision::Exact,
+crates/solver/src/gpu/mod.rs:59-62). That path performs the reference's
+floating-point operations in the reference's order, so the bar is
+bit-identical results:
 root values of single traversals, regrets and strategy sums after
 iterations, exploitability, and queries. The reference's own GPU-vs-CPU
 standard (crates/solver/src/gpu/engine/tests.rs:729-754, "exact mode
@@ -23,6 +25,11 @@ SPOTS = {
     "mid_street_raked": lambda: spots.mid_street_config(True),
     "mid_street": lambda: spots.mid_street_config(False),
 }
+
+
+def exact(cfg):
+    cfg.precision = abi.PRECISION_EXACT
+    return cfg
 
 
 def bits(a):
@@ -54,7 +61,7 @@ def random_storage(n, seed):
 def test_traversal_values_bit_identical(gpu, name):
     cfg = SPOTS[name]()
     o = OracleSolver(cfg)
-    g = Solver.new(cfg)
+    g = Solver.new(exact(cfg))
     assert g.storage_len() == len(o.storage()[0])
     r, s = random_storage(g.storage_len(), 7)
     for p in (0, 1):
@@ -75,7 +82,7 @@ def test_traversal_values_bit_identical(gpu, name):
 def test_five_iterations_bit_identical(gpu, name):
     cfg = SPOTS[name]()
     o = OracleSolver(cfg)
-    g = Solver.new(cfg)
+    g = Solver.new(exact(cfg))
     o.iterate(5)
     g.iterate(5)
     ro, so = o.storage()
@@ -90,7 +97,7 @@ def test_river_workload_1000_iterations_bit_identical(gpu):
     """The river workload (Ks7s2dTh4c, 1000 iterations) end to end."""
     cfg = workloads.river_spot()
     o = OracleSolver(cfg)
-    g = Solver.new(cfg)
+    g = Solver.new(exact(cfg))
     o.iterate(1000)
     g.iterate(1000)
     ro, so = o.storage()
@@ -107,7 +114,7 @@ def test_random_river_spots_bit_identical(gpu, seed):
         o = OracleSolver(cfg)
     except Exception:
         pytest.skip("spot rejected by Solver::new")
-    g = Solver.new(cfg)
+    g = Solver.new(exact(cfg))
     o.iterate(6)
     g.iterate(6)
     ro, so = o.storage()
@@ -121,7 +128,7 @@ def test_random_river_spots_bit_identical(gpu, seed):
 def test_queries_match(gpu, name):
     cfg = SPOTS[name]()
     o = OracleSolver(cfg)
-    g = Solver.new(cfg)
+    g = Solver.new(exact(cfg))
     o.iterate(8)
     g.iterate(8)
     paths = [[]]
