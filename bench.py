@@ -1,0 +1,391 @@
+#!/usr/bin/env python3
+"""DCFR solve benchmark on B200.
+
+Workload (default): the turn subgame Ks7s2dTh, 48 river runouts, pot 20bb,
+stacks 90bb, 33%/75%/all-in bets and one 2.5x raise on turn and river, ranges
+with class weights U[0,1) from seeds 1000/1001 and 51 of the 169 classes
+zeroed, f32 storage, DCFR alpha 1.5 beta 0 gamma 2. A step is one DCFR
+iteration (both traversals); the metric is DCFR iterations per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs as one process per GPU (torchrun): every rank solves its own copy
+of the spot (independent replicas, no collective on the data path); the
+timed region is bracketed by a barrier and a device synchronize on every
+rank, and the job time is the maximum over ranks.
+
+--impl reference times the CPU restatement of the reference's solver (the
+C++ oracle; the Rust reference cannot be built here) on this host's cores, on
+the same workload and metric; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import datetime as dt
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "time to 0.5%-pot exploitability, DCFR iters/s, % HBM roofline, vs CPU ref"
+UNIT = "DCFR iters/s"
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 1024 * 1024
+CLOCK_FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+WORKLOADS = {
+    "turn": ("turn subgame Ks7s2dTh: 48 river runouts, pot 20bb, stacks 90bb, bets 33%/75%/all-in + 2.5x raise "
+             "on turn and river, seeded class ranges (seeds 1000/1001, 51 of 169 classes zeroed), f32 storage, "
+             "DCFR alpha 1.5 beta 0 gamma 2"),
+    "river": ("river subgame Ks7s2dTh4c: pot 20bb, stacks 90bb, bets 50%/100%/all-in + 2.5x raise, seeded class "
+              "ranges (seeds 1000/1001), f32 storage, DCFR alpha 1.5 beta 0 gamma 2"),
+}
+
+
+def workload_config(name: str, precision: str):
+    from poker_trainer_b200 import workloads
+    cfg = workloads.turn_spot() if name == "turn" else workloads.river_spot()
+    from poker_trainer_b200 import abi
+    cfg.precision = abi.PRECISIONS[precision]
+    return cfg
+
+
+# ----------------------------------------------------------------- CPU oracle
+def oracle_lib():
+    """The CPU oracle (test infrastructure): used only for the CPU baseline and
+    the reference arm."""
+    path = os.path.join(HERE, "oracle", "liboracle.so")
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "oracle")], check=True)
+    L = C.CDLL(path)
+    L.oracle_create.restype = C.c_void_p
+    L.oracle_create.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    L.oracle_destroy.argtypes = [C.c_void_p]
+    L.oracle_iterate.argtypes = [C.c_void_p, C.c_uint32]
+    L.oracle_set_threads.argtypes = [C.c_int]
+    L.oracle_get_threads.restype = C.c_int
+    L.oracle_exploitability.argtypes = [C.c_void_p]
+    L.oracle_exploitability.restype = C.c_double
+    return L
+
+
+def time_oracle(cfg, threads: int, warmup: int, max_steps: int | None, budget_s: float | None):
+    """Iterations/s of the oracle on `threads` host threads: `warmup`
+    untimed iterations, then up to `max_steps` iterations or until `budget_s`
+    seconds have passed."""
+    L = oracle_lib()
+    L.oracle_set_threads(threads)
+    err = C.c_int(0)
+    h = L.oracle_create(C.byref(cfg), C.byref(err))
+    if not h:
+        raise RuntimeError(f"oracle_create failed ({err.value})")
+    try:
+        if warmup:
+            L.oracle_iterate(h, warmup)
+        done = 0
+        t0 = time.perf_counter()
+        while True:
+            L.oracle_iterate(h, 1)
+            done += 1
+            el = time.perf_counter() - t0
+            if max_steps is not None and done >= max_steps:
+                break
+            if budget_s is not None and el >= budget_s:
+                break
+        return done, el, L.oracle_get_threads()
+    finally:
+        L.oracle_destroy(h)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of one GPU during the timed region."""
+
+    def __init__(self, device_index: int):
+        import torch
+        ident = str(device_index)
+        try:
+            ident = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
+        except Exception:
+            pass
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={ident}", f"--query-gpu={CLOCK_FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        self.t0 = self.t1 = None
+
+    def begin(self):
+        self.t0 = dt.datetime.now()
+
+    def end(self):
+        self.t1 = dt.datetime.now()
+
+    def close(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [ln.strip() for ln in self.file.read().splitlines() if ln.strip()]
+        os.unlink(self.file.name)
+        samples = []
+        for ln in rows:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 10:
+                continue
+            try:
+                ts = dt.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                samples.append((ts, float(f[2]), float(f[3]), f[6:10]))
+            except ValueError:
+                continue
+        inside = [s for s in samples if self.t0 is not None and self.t0 <= s[0] <= self.t1]
+        use = inside or samples
+        if not use:
+            return None
+        reasons = sorted({REASONS[i] for s in use for i in range(4) if s[3][i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(s[1] for s in use), "sm_max_mhz": max(s[2] for s in use),
+                "reasons": reasons, "samples": len(use), "samples_in_timed_region": len(inside)}
+
+
+# ----------------------------------------------------------------- helpers
+def measured_peak():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    profiles/<kernel>_<workload>.md (a line 'traffic_bytes_per_launch: X')."""
+    path = os.path.join(HERE, "profiles", f"{kernel}_{workload}.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(ln.split(":", 1)[1].strip().split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+KERNEL_NAMES = {"terminal": "fast_terminal_kernel", "down": "down_kernel", "up": "up_kernel", "other": "other"}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------- arms
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    from poker_trainer_b200 import abi  # noqa: F401  (config layout only)
+    cfg = workload_config(args.workload, args.precision)
+    threads = os.cpu_count() or 1
+    steps, secs, used = time_oracle(cfg, threads, args.warmup, args.steps, args.reference_budget_s)
+    value = steps / secs
+    sample = f"{steps} DCFR iterations after {args.warmup} untimed ({args.workload} workload)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload], "parallelism": "host threads",
+                   "implementation": "CPU restatement of the reference's Rust solver (oracle/, C++ with OpenMP "
+                                     "over chance children); the Rust crate cannot be built here"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from poker_trainer_b200 import abi
+    from poker_trainer_b200.solver import Solver
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=dt.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def reduce(x: float, op: str) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX if op == "max" else pg.ReduceOp.SUM)
+        return float(t.item())
+
+    cfg = workload_config(args.workload, args.precision)
+    K, W = args.steps, args.warmup
+
+    # End to end through the public API: host config in, a K-iteration solve,
+    # the storage (regrets and strategy sums) read back into pinned host memory.
+    warm = Solver.new(cfg)  # CUDA context, module load
+    n_store = warm.storage_len()
+    warm.iterate(W)
+    warm.close()
+    pin_r = torch.empty(n_store, dtype=torch.float32, pin_memory=True)
+    pin_s = torch.empty(n_store, dtype=torch.float32, pin_memory=True)
+    out = (pin_r.numpy(), pin_s.numpy())
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_solver = Solver.new(cfg)
+    e2e_solver.iterate(K)
+    e2e_solver.download_storage(out=out)
+    t1 = time.perf_counter()
+    e2e_solver.close()
+    e2e_s = reduce(t1 - t0, "max")
+    h2d = C.sizeof(cfg)
+    d2h = 8 * n_store
+
+    # Device-resident solve: W warm-up iterations, then K timed iterations.
+    g = Solver.new(cfg)
+    g.iterate(W)
+    g.synchronize()
+    sampler = ClockSampler(local) if rank == 0 else None
+    time.sleep(0.5)
+    l0 = g.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    g.synchronize()
+    if sampler:
+        sampler.begin()
+    prof = g.iterate_profiled(K)
+    g.synchronize()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.end()
+    barrier()
+    launches = reduce(float(g.kernel_launches() - l0), "sum")
+    clocks = sampler.close() if sampler else None
+    ms = reduce(prof["total_ms"], "max")
+    # Unprofiled graph launches of the same iterations, for comparison.
+    g.iterate(K)
+    plain_ms = reduce(g.last_iterate_ms(), "max")
+    expl = g.exploitability()
+    pot = float(cfg.root.pot)
+    it_bytes = g.iteration_bytes()
+    g.close()
+
+    value = world * K / (ms / 1000.0)
+    peak, peak_kind = measured_peak()
+    classes = prof["classes"]
+    dom = max(("down", "terminal", "up"), key=lambda c: classes[c]["ms"])
+    dc = classes[dom]
+    per_launch_ms = dc["ms"] / max(dc["launches"], 1)
+    per_launch_bytes = dc["bytes"] / max(dc["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
+    kernels = {c: {"launches": v["launches"], "ms": v["ms"], "share": v["ms"] / max(prof["total_ms"], 1e-12),
+                   "gbs": (v["bytes"] / (v["ms"] / 1000.0) / 1e9) if v["ms"] > 0 else None}
+               for c, v in classes.items()}
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+
+    # CPU baseline: the oracle on this host's cores, a bounded sample.
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        steps, secs, used = time_oracle(cfg, threads, 2, None, args.cpu_budget_s)
+        cpu = {"value": steps / secs, "unit": UNIT, "cores": used, "kind": "port",
+               "sample": f"{steps} DCFR iterations of the same workload after 2 untimed, {secs:.1f} s on {used} "
+                         f"host threads (C++ restatement of the reference's CPU solver)"}
+
+    working = it_bytes
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": WORKLOADS[args.workload], "iterations_per_step": 1, "precision": args.precision,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": (f"inputs larger than L2: one iteration moves {working / 1e6:.0f} MB of rows and storage "
+                   f"(> {L2_BYTES / 1e6:.0f} MB L2), no flush") if working > L2_BYTES else
+                  "working set smaller than L2 (no flush; L2-resident figure)",
+            "timing": "CUDA events on the solver's stream around every kernel class, inside the captured "
+                      "iteration graph; max over ranks",
+        },
+        "clocks": clocks,
+        "e2e": {"value": world * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "what": "dcfr_create from the host config + K iterations + regrets and sums read back into pinned "
+                        "host memory, wall clock, max over ranks; bytes are the per-solve totals / K"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom] if args.precision == "fast" or dom != "terminal"
+                     else "terminal_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
+                     "traffic": ncu_traffic(KERNEL_NAMES[dom], args.workload),
+                     "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
+        "iteration_roofline": {"bytes_per_iteration": it_bytes,
+                               "achieved": it_bytes * (K / (ms / 1000.0)) / 1e9, "peak": peak, "unit": "GB/s",
+                               "frac": it_bytes * (K / (ms / 1000.0)) / 1e9 / peak},
+        "kernels": kernels,
+        "unprofiled_ms_per_step": plain_ms / K,
+        "exploitability_pct_after": 100.0 * expl / pot,
+        "iterations_after": W + 2 * K,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="turn")
+    ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--cpu-budget-s", type=float, default=10.0)
+    ap.add_argument("--reference-budget-s", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -298,6 +298,29 @@ int dcfr_kernel_launches(const dcfr_solver* s, uint64_t* out);
 int dcfr_last_iterate_ms(dcfr_solver* s, double* ms);
 int dcfr_iteration_bytes(const dcfr_solver* s, double* bytes);
 
+/* Kernel classes of one traversal: down levels (opponent and chance
+ * splits), the terminal launch, up levels (own-node updates, opponent and
+ * chance sums), and everything else (discount advance, row resets, the gaps
+ * between graph launches). */
+enum { DCFR_KERNEL_DOWN = 0, DCFR_KERNEL_TERMINAL = 1, DCFR_KERNEL_UP = 2, DCFR_KERNEL_OTHER = 3 };
+#define DCFR_KERNEL_CLASSES 4
+
+typedef struct dcfr_kernel_profile {
+  uint32_t iterations;
+  uint32_t _pad;
+  uint64_t launches[DCFR_KERNEL_CLASSES]; /* kernel launches per class */
+  double ms[DCFR_KERNEL_CLASSES];         /* summed device time per class */
+  double bytes[DCFR_KERNEL_CLASSES];      /* compulsory bytes per class: rows read and
+                                             written, storage read and written */
+  double total_ms;                        /* first to last event */
+} dcfr_kernel_profile;
+
+/* Measurement hook, no counterpart in the reference: runs `iterations` DCFR
+ * iterations (they advance the solve exactly as dcfr_iterate's) from a second
+ * captured graph that also records a CUDA event on the handle's stream at
+ * every class boundary, and returns the per-class totals. */
+int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profile* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,6 +115,20 @@ class Config(C.Structure):
     ]
 
 
+KERNEL_CLASSES = ("down", "terminal", "up", "other")  # DCFR_KERNEL_* order
+
+
+class KernelProfile(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint32),
+        ("_pad", C.c_uint32),
+        ("launches", C.c_uint64 * 4),
+        ("ms", C.c_double * 4),
+        ("bytes", C.c_double * 4),
+        ("total_ms", C.c_double),
+    ]
+
+
 class TreeStats(C.Structure):
     _fields_ = [
         ("player_nodes", C.c_uint64),

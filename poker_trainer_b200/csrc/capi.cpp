@@ -332,4 +332,12 @@ int dcfr_iteration_bytes(const dcfr_solver* s, double* bytes) {
   return DCFR_OK;
 }
 
+int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profile* out) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");
+  GUARD_BEGIN
+  return done(s->e->iterate_profiled(iterations, *out));
+  GUARD_END
+}
+
 }  // extern "C"

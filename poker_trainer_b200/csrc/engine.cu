@@ -149,6 +149,7 @@ Engine::~Engine() {
   dfree(disc_table_);
   dfree(cur_disc_);
   dfree(counter_);
+  for (cudaEvent_t e : prof_events_) cudaEventDestroy(e);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -159,6 +160,11 @@ void Engine::free_graphs() {
   if (br_graph_) cudaGraphExecDestroy(br_graph_);
   if (avg_graph_) cudaGraphExecDestroy(avg_graph_);
   iter_graph_ = br_graph_ = avg_graph_ = nullptr;
+  if (prof_exec_) cudaGraphExecDestroy(prof_exec_);
+  if (prof_graph_) cudaGraphDestroy(prof_graph_);
+  prof_exec_ = nullptr;
+  prof_graph_ = nullptr;
+  marks_.clear();
 }
 
 int Engine::isomorphic_pairs() const {
@@ -543,8 +549,26 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   int kernels = 0;
   for (auto& l : plan.down) kernels += l.count > 0;
   for (auto& l : plan.up) kernels += l.count > 0;
-  kernels += fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
+  const int term_kernels = fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
+  kernels += term_kernels;
   plan.kernels = kernels;
+  // Per class: launches and compulsory bytes of one CFR traversal (rows of
+  // n floats, f32 storage).
+  for (int c = 0; c < DCFR_KERNEL_CLASSES; c++) {
+    plan.class_kernels[c] = 0;
+    plan.class_bytes[c] = 0.0;
+  }
+  for (auto& l : plan.down) plan.class_kernels[DCFR_KERNEL_DOWN] += l.count > 0;
+  for (auto& l : plan.up) plan.class_kernels[DCFR_KERNEL_UP] += l.count > 0;
+  plan.class_kernels[DCFR_KERNEL_TERMINAL] = term_kernels;
+  const double np_ = g.n[p], no_ = g.n[o];
+  for (const DownTask& t : plan.h_down)
+    plan.class_bytes[DCFR_KERNEL_DOWN] +=
+        t.kind == D_OPP_SPLIT ? 4.0 * no_ * (1.0 + 4.0 * t.nchild) : 4.0 * no_ * (1.0 + t.nchild);
+  for (const UpTask& t : plan.h_up)
+    plan.class_bytes[DCFR_KERNEL_UP] += t.kind == U_OWN ? 4.0 * np_ * (3.0 * t.nchild + 1.0) : 4.0 * np_ * (t.nchild + 1.0);
+  for (const TermLane& L : plan.h_lanes)
+    plan.class_bytes[DCFR_KERNEL_TERMINAL] += 4.0 * (no_ + np_) + (L.frow != NONE32 ? 4.0 * np_ : 0.0);
   return Status();
 }
 
@@ -649,12 +673,14 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   cudaMemsetAsync(alive_, 0, (size_t)plan.nslots * 4, stream_);
   cudaMemsetAsync(alive_, 1, 4, stream_);
   cudaMemcpyAsync(reach_, root_row, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice, stream_);
+  mark(DCFR_KERNEL_OTHER);
   RowArgs A;
   row_args(p, A);
   const int dchunks = (hp_[o] + ROW_CHUNK - 1) / ROW_CHUNK;
   const int uchunks = (hp_[p] + ROW_CHUNK - 1) / ROW_CHUNK;
   for (const Plan::Level& l : plan.down)
     if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, dchunks, stream_);
+  mark(DCFR_KERNEL_DOWN);
   if (fast_) {
     if (!plan.h_fast.empty()) {
       FastArgs F;
@@ -667,10 +693,12 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
     for (const Plan::Wave& w : plan.waves)
       launch_terminal(T, plan.d_groups, plan.d_lanes, plan.d_tasks + w.first, (int)w.count, stream_);
   }
+  mark(DCFR_KERNEL_TERMINAL);
   for (size_t d = plan.up.size(); d-- > 0;) {
     const Plan::Level& l = plan.up[d];
     if (l.count) launch_up(mode, l.maxa, A, plan.d_up + l.first, (int)l.count, uchunks, stream_);
   }
+  mark(DCFR_KERNEL_UP);
   if (root_out)
     cudaMemcpyAsync(root_out, vals_ + (size_t)plan.root * stride_, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice,
                     stream_);
@@ -713,6 +741,89 @@ Status Engine::capture_graphs() {
     cudaGraphDestroy(graph);
   }
   pair_kernels_ = full_[0]->kernels + full_[1]->kernels;
+  return Status();
+}
+
+// Records an event-record node into the profiled graph being captured and
+// remembers it with the class of the interval it closes.
+void Engine::mark(int cls) {
+  if (!marking_ || !mark_status_.ok()) return;
+  // An external event record becomes a graph node (a plain record inside a
+  // capture only orders streams).
+  cudaError_t e = cudaEventRecordWithFlags(ev0_, stream_, cudaEventRecordExternal);
+  cudaStreamCaptureStatus st;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(stream_, &st, nullptr, nullptr, &deps, &ndeps);
+  if (e != cudaSuccess || ndeps != 1) {
+    mark_status_ = e != cudaSuccess ? cuda_status(e, "profiled graph capture") : Status{DCFR_ERR_CUDA, "profiled graph capture: unexpected dependencies"};
+    return;
+  }
+  marking_->push_back(Mark{deps[0], cls});
+}
+
+// One DCFR iteration as in capture_graphs, with an event at the start and at
+// every kernel-class boundary.
+Status Engine::capture_profiled_graph() {
+  if (prof_exec_) return Status();
+  marks_.clear();
+  mark_status_ = Status();
+  marking_ = &marks_;
+  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  mark(-1);
+  launch_advance(counter_, disc_table_, disc_len_, cur_disc_, stream_);
+  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr);
+  enqueue_traversal(*full_[1], M_CFR, root_rows_ + stride_, nullptr);
+  marking_ = nullptr;
+  cudaError_t e = cudaStreamEndCapture(stream_, &prof_graph_);
+  if (!mark_status_.ok()) return mark_status_;
+  CK(e);
+  CK(cudaGraphInstantiate(&prof_exec_, prof_graph_, 0));
+  return Status();
+}
+
+Status Engine::iterate_profiled(uint32_t n, dcfr_kernel_profile& out) {
+  std::memset(&out, 0, sizeof out);
+  Status s;
+  if (!(s = ensure_discounts(iterations + n + 1)).ok()) return s;
+  if (!(s = capture_graphs()).ok()) return s;
+  if (!(s = capture_profiled_graph()).ok()) return s;
+  const size_t M = marks_.size();
+  while (prof_events_.size() < (size_t)n * M) {
+    cudaEvent_t ev;
+    CK(cudaEventCreate(&ev));
+    prof_events_.push_back(ev);
+  }
+  for (uint32_t i = 0; i < n; i++) {
+    for (size_t m = 0; m < M; m++)
+      CK(cudaGraphExecEventRecordNodeSetEvent(prof_exec_, marks_[m].node, prof_events_[(size_t)i * M + m]));
+    CK(cudaGraphLaunch(prof_exec_, stream_));
+    launches += iter_kernels_;
+  }
+  iterations += n;
+  CK(cudaStreamSynchronize(stream_));
+  out.iterations = n;
+  for (uint32_t i = 0; i < n; i++)
+    for (size_t m = 0; m < M; m++) {
+      const size_t k = (size_t)i * M + m;
+      if (k == 0) continue;
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, prof_events_[k - 1], prof_events_[k]));
+      // The first event of an iteration closes the gap after the previous one.
+      const int cls = m == 0 ? DCFR_KERNEL_OTHER : marks_[m].cls;
+      out.ms[cls] += ms;
+    }
+  if (n > 0) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, prof_events_[0], prof_events_[(size_t)n * M - 1]));
+    out.total_ms = ms;
+    last_iterate_ms = ms;
+  }
+  for (int c = 0; c < DCFR_KERNEL_CLASSES; c++) {
+    out.launches[c] = (uint64_t)n * (full_[0]->class_kernels[c] + full_[1]->class_kernels[c]);
+    out.bytes[c] = (double)n * (full_[0]->class_bytes[c] + full_[1]->class_bytes[c]);
+  }
+  out.launches[DCFR_KERNEL_OTHER] += n;  // the discount advance
   return Status();
 }
 

@@ -75,6 +75,8 @@ struct Plan {
   TermLane* d_lanes = nullptr;
   FastTask* d_fast = nullptr;
   int kernels = 0;  // kernel launches per traversal
+  int class_kernels[DCFR_KERNEL_CLASSES] = {0, 0, 0, 0};
+  double class_bytes[DCFR_KERNEL_CLASSES] = {0, 0, 0, 0};  // compulsory bytes per traversal (CFR mode)
   uint64_t nodes = 0;
   ~Plan();
 };
@@ -91,6 +93,7 @@ class Engine {
   double last_iterate_ms = 0.0;
 
   Status iterate(uint32_t n);
+  Status iterate_profiled(uint32_t n, dcfr_kernel_profile& out);
   Status sync();
   Status exploitability(double& out);
   Status root_values(double out[2]);
@@ -157,6 +160,19 @@ class Engine {
   std::vector<uint32_t> cc_off_, iso_first_;
   std::unique_ptr<Plan> full_[2];
   cudaGraphExec_t iter_graph_ = nullptr, br_graph_ = nullptr, avg_graph_ = nullptr;
+  // Profiled iteration graph: event-record nodes at kernel-class boundaries.
+  struct Mark {
+    cudaGraphNode_t node;
+    int cls;  // class of the interval that ends at this event (-1: first)
+  };
+  std::vector<Mark>* marking_ = nullptr;  // set while capturing the profiled graph
+  cudaGraph_t prof_graph_ = nullptr;
+  cudaGraphExec_t prof_exec_ = nullptr;
+  std::vector<Mark> marks_;
+  std::vector<cudaEvent_t> prof_events_;
+  Status mark_status_;
+  void mark(int cls);
+  Status capture_profiled_graph();
   int iter_kernels_ = 0, pair_kernels_ = 0;
 
   Status init();

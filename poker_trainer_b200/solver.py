@@ -28,7 +28,7 @@ EXPORTS = [
     "dcfr_last_exploitability", "dcfr_stats", "dcfr_isomorphic_pairs", "dcfr_hands", "dcfr_is_decision",
     "dcfr_actions_at", "dcfr_query_sizes", "dcfr_query", "dcfr_ranges_after", "dcfr_storage_len",
     "dcfr_download_storage", "dcfr_upload_storage", "dcfr_set_iterations", "dcfr_traverse",
-    "dcfr_kernel_launches", "dcfr_last_iterate_ms", "dcfr_iteration_bytes",
+    "dcfr_kernel_launches", "dcfr_last_iterate_ms", "dcfr_iteration_bytes", "dcfr_iterate_profiled",
 ]
 
 
@@ -69,6 +69,7 @@ def lib():
         L.dcfr_kernel_launches.argtypes = [P, C.POINTER(C.c_uint64)]
         L.dcfr_last_iterate_ms.argtypes = [P, C.POINTER(C.c_double)]
         L.dcfr_iteration_bytes.argtypes = [P, C.POINTER(C.c_double)]
+        L.dcfr_iterate_profiled.argtypes = [P, C.c_uint32, C.POINTER(abi.KernelProfile)]
         _lib = L
     return _lib
 
@@ -339,10 +340,20 @@ class Solver:
         check(lib().dcfr_storage_len(self._h, C.byref(x)))
         return x.value
 
-    def download_storage(self):
+    def download_storage(self, out=None):
+        """Regrets and strategy sums (the reference's HostStorage). `out` may
+        supply two contiguous float32 arrays of storage_len() (for instance
+        views of pinned host memory)."""
         n = self.storage_len()
-        r = np.zeros(n, np.float32)
-        s = np.zeros(n, np.float32)
+        if out is None:
+            r = np.zeros(n, np.float32)
+            s = np.zeros(n, np.float32)
+        else:
+            r, s = out
+            if r.dtype != np.float32 or s.dtype != np.float32 or len(r) < n or len(s) < n:
+                raise ValueError("out arrays must be float32 with storage_len() entries")
+            if not (r.flags.c_contiguous and s.flags.c_contiguous):
+                raise ValueError("out arrays must be contiguous")
         check(lib().dcfr_download_storage(self._h, _ptr(r), _ptr(s), n))
         return r, s
 
@@ -373,3 +384,14 @@ class Solver:
         x = C.c_double()
         check(lib().dcfr_iteration_bytes(self._h, C.byref(x)))
         return x.value
+
+    def iterate_profiled(self, n: int) -> dict:
+        """Runs n iterations with CUDA events at every kernel-class boundary;
+        returns per class (down, terminal, up, other) launches, device ms and
+        compulsory bytes, plus the first-to-last-event total."""
+        prof = abi.KernelProfile()
+        check(lib().dcfr_iterate_profiled(self._h, n, C.byref(prof)))
+        classes = {}
+        for c, name in enumerate(abi.KERNEL_CLASSES):
+            classes[name] = dict(launches=int(prof.launches[c]), ms=float(prof.ms[c]), bytes=float(prof.bytes[c]))
+        return dict(iterations=int(prof.iterations), total_ms=float(prof.total_ms), classes=classes)
