@@ -53,6 +53,9 @@ Plan::~Plan() {
   dfree(d_lanes);
   dfree(d_tasks);
   dfree(d_fast);
+  dfree(d_trees);
+  dfree(d_fdown);
+  dfree(d_fup);
 }
 
 // DcfrParams -> Discount (cfr.rs:86-106), host f64 pow as the reference.
@@ -308,7 +311,13 @@ Status Engine::init() {
       int dev = 0, sms = 0;
       CK(cudaGetDevice(&dev));
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      fast_blocks_ = sms * fast_blocks_per_sm(stride_, femax_);
+      const int per_sm = fast_blocks_per_sm(stride_, femax_, fcstride_, tstride_);
+      if (per_sm <= 0) {
+        s.code = DCFR_ERR_CUDA;
+        s.msg = "terminal kernel: shared-memory layout does not fit an SM";
+        return s;
+      }
+      fast_blocks_ = sms * per_sm;
     }
   }
   // Plans for the two traversals of an iteration.
@@ -377,6 +386,34 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // Slots of nodes in the subtree (node ids may be sparse for subtrees).
   std::unordered_map<uint32_t, uint32_t> slot;
   slot[root] = 0;
+  // Fused river subtrees (one block each, fused_*_kernel): river-street
+  // children of chance nodes, when there are enough to fill the GPU.
+  auto river_root = [&](uint32_t v) {
+    const GNode& nd = g.nodes[v];
+    return v != root && nd.kind == N_PLAYER && nd.street == DCFR_RIVER && nd.parent != NO &&
+           g.nodes[nd.parent].kind == N_CHANCE;
+  };
+  bool fuse = false;
+  {
+    size_t candidates = 0;
+    std::vector<uint32_t> st{root};
+    while (!st.empty()) {
+      uint32_t v = st.back();
+      st.pop_back();
+      if (river_root(v)) {
+        candidates++;
+        continue;
+      }
+      const GNode& nd = g.nodes[v];
+      if (nd.kind == N_PLAYER || nd.kind == N_CHANCE)
+        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back(nd.first + i);
+    }
+    fuse = candidates >= 64;
+  }
+  std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> tree_of;  // node -> (tree, depth in tree)
+  std::vector<std::vector<std::pair<uint32_t, DownTask>>> fdown;
+  std::vector<std::vector<std::pair<uint32_t, UpTask>>> fup;
+  int fmaxa = 0;
   q.push_back({root, 0});
   const double hp = g.half_pot, norm = g.norm;
   uint64_t count = 0;
@@ -386,7 +423,36 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     count++;
     const GNode& nd = g.nodes[v];
     const uint32_t sv = slot[v];
-    if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
+    uint32_t tree = NONE32, tdepth = 0;
+    if (fuse) {
+      if (river_root(v)) {
+        tree = (uint32_t)fdown.size();
+        fdown.emplace_back();
+        fup.emplace_back();
+      } else if (nd.parent != NO) {
+        auto it = tree_of.find(nd.parent);
+        if (it != tree_of.end()) {
+          tree = it->second.first;
+          tdepth = it->second.second + 1;
+        }
+      }
+      if (tree != NONE32) tree_of[v] = {tree, tdepth};
+    }
+    if (tree != NONE32 && nd.kind == N_PLAYER) {
+      // Inside a fused river subtree (no chance nodes below the river).
+      bool own = nd.player == p;
+      uint32_t first_slot = own ? sv : next_slot;
+      if (!own) next_slot += nd.nchild;
+      for (uint32_t i = 0; i < nd.nchild; i++) {
+        uint32_t c = nd.first + i;
+        slot[c] = own ? sv : first_slot + i;
+        q.push_back({c, depth + 1});
+      }
+      if (!own) fdown[tree].push_back({tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f}});
+      fup[tree].push_back({tdepth, UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
+                                          first_slot, gpu_off_[v], 0, 0, 0, 0}});
+      fmaxa = std::max<int>(fmaxa, (int)nd.nchild);
+    } else if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
       if (down.size() <= depth) {
         down.resize(depth + 1);
         up.resize(depth + 1);
@@ -471,15 +537,45 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   }
   plan.nodes = count;
   plan.nslots = next_slot;
+  // Fused subtrees: down tasks in BFS order with a barrier at each new level,
+  // up tasks deepest level first.
+  plan.h_trees.clear();
+  plan.h_fdown.clear();
+  plan.h_fup.clear();
+  plan.fused_maxa = fmaxa;
+  for (size_t t = 0; t < fdown.size(); t++) {
+    FusedTree F{(uint32_t)plan.h_fdown.size(), 0, (uint32_t)plan.h_fup.size(), 0};
+    uint32_t prev = 0;
+    for (size_t i = 0; i < fdown[t].size(); i++) {
+      DownTask T = fdown[t][i].second;
+      if (i > 0 && fdown[t][i].first != prev) T.kind |= LEVEL_BREAK;
+      prev = fdown[t][i].first;
+      plan.h_fdown.push_back(T);
+    }
+    std::stable_sort(fup[t].begin(), fup[t].end(),
+                     [](const std::pair<uint32_t, UpTask>& a, const std::pair<uint32_t, UpTask>& b) {
+                       return a.first > b.first;
+                     });
+    for (auto& x : fup[t]) plan.h_fup.push_back(x.second);
+    F.down_count = (uint32_t)(plan.h_fdown.size() - F.down_first);
+    F.up_count = (uint32_t)(plan.h_fup.size() - F.up_first);
+    plan.h_trees.push_back(F);
+  }
   // Flatten levels.
   plan.h_down.clear();
   plan.h_up.clear();
   plan.down.assign(down.size(), Plan::Level());
   plan.up.assign(up.size(), Plan::Level());
+  // Within a level, tasks by kind (one launch per kind present).
   for (size_t d = 0; d < down.size(); d++) {
-    plan.down[d] = Plan::Level{(uint32_t)plan.h_down.size(), (uint32_t)down[d].size(), dmax[d]};
+    std::stable_sort(down[d].begin(), down[d].end(),
+                     [](const DownTask& a, const DownTask& b) { return a.kind < b.kind; });
+    std::stable_sort(up[d].begin(), up[d].end(), [](const UpTask& a, const UpTask& b) { return a.kind < b.kind; });
+    plan.down[d] = Plan::Level{(uint32_t)plan.h_down.size(), (uint32_t)down[d].size(), dmax[d], {0, 0, 0}};
+    for (const DownTask& t : down[d]) plan.down[d].kind_count[t.kind]++;
     plan.h_down.insert(plan.h_down.end(), down[d].begin(), down[d].end());
-    plan.up[d] = Plan::Level{(uint32_t)plan.h_up.size(), (uint32_t)up[d].size(), umax[d]};
+    plan.up[d] = Plan::Level{(uint32_t)plan.h_up.size(), (uint32_t)up[d].size(), umax[d], {0, 0, 0}};
+    for (const UpTask& t : up[d]) plan.up[d].kind_count[t.kind]++;
     plan.h_up.insert(plan.h_up.end(), up[d].begin(), up[d].end());
   }
   // Terminal groups: showdowns by (kind, board), folds by kind, 32 lanes each.
@@ -549,6 +645,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   int kernels = 0;
   for (auto& l : plan.down) kernels += l.count > 0;
   for (auto& l : plan.up) kernels += l.count > 0;
+  if (!plan.h_trees.empty()) kernels += 2;
   const int term_kernels = fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
   kernels += term_kernels;
   plan.kernels = kernels;
@@ -560,13 +657,20 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   }
   for (auto& l : plan.down) plan.class_kernels[DCFR_KERNEL_DOWN] += l.count > 0;
   for (auto& l : plan.up) plan.class_kernels[DCFR_KERNEL_UP] += l.count > 0;
+  if (!plan.h_trees.empty()) {
+    plan.class_kernels[DCFR_KERNEL_DOWN]++;
+    plan.class_kernels[DCFR_KERNEL_UP]++;
+  }
   plan.class_kernels[DCFR_KERNEL_TERMINAL] = term_kernels;
   const double np_ = g.n[p], no_ = g.n[o];
-  for (const DownTask& t : plan.h_down)
-    plan.class_bytes[DCFR_KERNEL_DOWN] +=
-        t.kind == D_OPP_SPLIT ? 4.0 * no_ * (1.0 + 4.0 * t.nchild) : 4.0 * no_ * (1.0 + t.nchild);
-  for (const UpTask& t : plan.h_up)
-    plan.class_bytes[DCFR_KERNEL_UP] += t.kind == U_OWN ? 4.0 * np_ * (3.0 * t.nchild + 1.0) : 4.0 * np_ * (t.nchild + 1.0);
+  for (const std::vector<DownTask>* v : {&plan.h_down, &plan.h_fdown})
+    for (const DownTask& t : *v)
+      plan.class_bytes[DCFR_KERNEL_DOWN] += (t.kind & KIND_MASK) == D_OPP_SPLIT ? 4.0 * no_ * (1.0 + 4.0 * t.nchild)
+                                                                                : 4.0 * no_ * (1.0 + t.nchild);
+  for (const std::vector<UpTask>* v : {&plan.h_up, &plan.h_fup})
+    for (const UpTask& t : *v)
+      plan.class_bytes[DCFR_KERNEL_UP] +=
+          t.kind == U_OWN ? 4.0 * np_ * (3.0 * t.nchild + 1.0) : 4.0 * np_ * (t.nchild + 1.0);
   for (const TermLane& L : plan.h_lanes)
     plan.class_bytes[DCFR_KERNEL_TERMINAL] += 4.0 * (no_ + np_) + (L.frow != NONE32 ? 4.0 * np_ : 0.0);
   return Status();
@@ -580,6 +684,17 @@ Status Engine::upload_plan(Plan& plan) {
   if (!(s = dalloc(plan.d_lanes, plan.h_lanes.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_tasks, plan.h_tasks.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fast, plan.h_fast.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_trees, plan.h_trees.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_fdown, plan.h_fdown.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_fup, plan.h_fup.size(), "plan")).ok()) return s;
+  if (!plan.h_trees.empty()) {
+    CK(cudaMemcpy(plan.d_trees, plan.h_trees.data(), plan.h_trees.size() * sizeof(FusedTree), cudaMemcpyHostToDevice));
+    if (!plan.h_fdown.empty())
+      CK(cudaMemcpy(plan.d_fdown, plan.h_fdown.data(), plan.h_fdown.size() * sizeof(DownTask),
+                    cudaMemcpyHostToDevice));
+    if (!plan.h_fup.empty())
+      CK(cudaMemcpy(plan.d_fup, plan.h_fup.data(), plan.h_fup.size() * sizeof(UpTask), cudaMemcpyHostToDevice));
+  }
   if (!plan.h_fast.empty())
     CK(cudaMemcpy(plan.d_fast, plan.h_fast.data(), plan.h_fast.size() * sizeof(FastTask), cudaMemcpyHostToDevice));
   if (!plan.h_tasks.empty())
@@ -676,10 +791,9 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   mark(DCFR_KERNEL_OTHER);
   RowArgs A;
   row_args(p, A);
-  const int dchunks = (hp_[o] + ROW_CHUNK - 1) / ROW_CHUNK;
-  const int uchunks = (hp_[p] + ROW_CHUNK - 1) / ROW_CHUNK;
   for (const Plan::Level& l : plan.down)
-    if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, dchunks, stream_);
+    if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, hp_[o], stream_);
+  launch_fused_down(mode, plan.fused_maxa, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fdown, hp_[o], stream_);
   mark(DCFR_KERNEL_DOWN);
   if (fast_) {
     if (!plan.h_fast.empty()) {
@@ -694,9 +808,10 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
       launch_terminal(T, plan.d_groups, plan.d_lanes, plan.d_tasks + w.first, (int)w.count, stream_);
   }
   mark(DCFR_KERNEL_TERMINAL);
+  launch_fused_up(mode, plan.fused_maxa, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fup, hp_[p], stream_);
   for (size_t d = plan.up.size(); d-- > 0;) {
     const Plan::Level& l = plan.up[d];
-    if (l.count) launch_up(mode, l.maxa, A, plan.d_up + l.first, (int)l.count, uchunks, stream_);
+    if (l.count) launch_up(mode, l.maxa, A, plan.d_up + l.first, (int)l.count, hp_[p], stream_);
   }
   mark(DCFR_KERNEL_UP);
   if (root_out)

@@ -18,8 +18,12 @@ struct RowArgs;
 struct TermArgs;
 
 // Kernel launchers (kernels.cu).
-void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s);
-void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s);
+void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s);
+void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s);
+void launch_fused_down(int mode, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees,
+                       const DownTask* tasks, int hp, cudaStream_t s);
+void launch_fused_up(int mode, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees, const UpTask* tasks,
+                     int hp, cudaStream_t s);
 void launch_terminal(const TermArgs& A, const TermGroup* groups, const TermLane* lanes, const TermTask* tasks,
                      int ntasks, cudaStream_t s);
 cudaError_t terminal_kernel_setup();
@@ -36,7 +40,7 @@ void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstrid
                          uint16_t* cat, uint16_t* seg, uint4* rec, int cstride, cudaStream_t s);
 void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
 int fast_emax(int tstride);
-int fast_blocks_per_sm(int stride, int emax);
+int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride);
 void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
 void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
 void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
@@ -53,9 +57,11 @@ struct Plan {
   int p = 0;
   uint32_t root = 0;
   uint32_t nslots = 0;
+  // A level's tasks, sorted by kind: count[k] tasks of kind k from first on.
   struct Level {
     uint32_t first = 0, count = 0;
     int maxa = 0;
+    uint32_t kind_count[3] = {0, 0, 0};
   };
   std::vector<Level> down, up;  // up[d] for depth d (launched deepest first)
   std::vector<DownTask> h_down;
@@ -64,6 +70,14 @@ struct Plan {
   std::vector<TermLane> h_lanes;
   std::vector<TermTask> h_tasks;
   std::vector<FastTask> h_fast;  // fast precision: one task per terminal
+  // Fused river subtrees (one block each) and their tasks.
+  std::vector<FusedTree> h_trees;
+  std::vector<DownTask> h_fdown;
+  std::vector<UpTask> h_fup;
+  int fused_maxa = 0;
+  FusedTree* d_trees = nullptr;
+  DownTask* d_fdown = nullptr;
+  UpTask* d_fup = nullptr;
   struct Wave {
     uint32_t first = 0, count = 0, groups = 0;
   };

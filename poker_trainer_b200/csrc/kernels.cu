@@ -28,32 +28,45 @@ __device__ __forceinline__ float recipf(float d) {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float& at(float4& v, int j) { return (&v.x)[j]; }
+// Per-player fields of the kernel arguments, selected without indexing the
+// parameter arrays (a dynamic index would copy them to local memory).
+template <typename T>
+__device__ __forceinline__ T pick(int q, const T (&v)[2]) {
+  return q ? v[1] : v[0];
+}
+
 __device__ __forceinline__ bool nz4(const float4& v) { return v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f; }
 
 // ------------------------------------------------------------- down levels
 // Opponent split (cfr.rs:384-420 / river.rs:115-160) and chance split
 // (cfr.rs:448-456).
-template <int MODE, int MAXA>
-__global__ void __launch_bounds__(ROW_THREADS) down_kernel(RowArgs A, const DownTask* __restrict__ tasks, int chunks) {
-  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
-  const DownTask T = tasks[t];
-  if (A.alive[T.in_slot] == 0) return;  // dead subtree: children stay dead
+// One warp's item: hands [h0, h0 + 128) of one node, 4 per lane.
+template <int MODE, int MAXA, int KIND>
+__device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, int h0, int lane) {
+  const uint32_t live = A.alive[T.in_slot];
+  if (live == 0) return;  // dead subtree: children stay dead
   const int o = A.p ^ 1;
-  const int hp = A.hp[o];
-  const int h0 = ch * ROW_CHUNK + threadIdx.x * VEC;
+  const int hp = pick(o, A.hp);
   const bool valid = h0 < hp;
-  const int lane = threadIdx.x & 31;
   const size_t stride = (size_t)A.stride;
   float4 r = valid ? ld4(A.reach + (size_t)T.in_slot * stride + h0) : make_float4(0.f, 0.f, 0.f, 0.f);
-  if (T.kind == D_OPP_SPLIT) {
+  if constexpr (KIND == D_OPP_SPLIT) {
     const int na = (int)T.nchild;
     const float uniform = 1.0f / (float)na;
     float4 x[MAXA];
     float4 inv;
     const float* base = (MODE == M_CFR ? A.regrets : A.sums) + T.store + h0;
+    float* sb = A.sums + T.store + h0;
+    float4 sums[MODE == M_CFR ? MAXA : 1];
+    // Every storage load of the node is issued before the arithmetic.
 #pragma unroll
     for (int a = 0; a < MAXA; a++)
       if (a < na) x[a] = valid ? ld4(base + (size_t)a * hp) : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (MODE == M_CFR) {
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na && valid) sums[a] = ld4(sb + (size_t)a * hp);
+    }
     if (MODE == M_CFR) {
       // regret_match_into (cfr.rs:161-192).
 #pragma unroll
@@ -71,11 +84,10 @@ __global__ void __launch_bounds__(ROW_THREADS) down_kernel(RowArgs A, const Down
           for (int j = 0; j < VEC; j++) at(x[a], j) = at(inv, j) == 0.0f ? uniform : max0(at(x[a], j)) * at(inv, j);
       // Strategy sums s*gamma + sigma (or + sigma*reach) (cfr.rs:395-407).
       const DiscountD d = *A.disc;
-      float* sb = A.sums + T.store + h0;
 #pragma unroll
       for (int a = 0; a < MAXA; a++)
         if (a < na && valid) {
-          float4 s = ld4(sb + (size_t)a * hp);
+          float4 s = sums[MODE == M_CFR ? a : 0];
 #pragma unroll
           for (int j = 0; j < VEC; j++) {
             float add = d.reach_weighted ? at(x[a], j) * at(r, j) : at(x[a], j);
@@ -114,8 +126,8 @@ __global__ void __launch_bounds__(ROW_THREADS) down_kernel(RowArgs A, const Down
     // Chance split: reach*factor, opponent hands holding the card zeroed.
     uchar4 oc1 = make_uchar4(255, 255, 255, 255), oc2 = oc1;
     if (valid) {
-      oc1 = *reinterpret_cast<const uchar4*>(A.hc1[o] + h0);
-      oc2 = *reinterpret_cast<const uchar4*>(A.hc2[o] + h0);
+      oc1 = *reinterpret_cast<const uchar4*>(pick(o, A.hc1) + h0);
+      oc2 = *reinterpret_cast<const uchar4*>(pick(o, A.hc2) + h0);
     }
     const uint8_t* cards = A.chance_cards + T.cards;
     for (uint32_t i = 0; i < T.nchild; i++) {
@@ -136,23 +148,30 @@ __global__ void __launch_bounds__(ROW_THREADS) down_kernel(RowArgs A, const Down
 // --------------------------------------------------------------- up levels
 // Traverser node (own_node_update, cfr.rs:315-382), opponent node sum
 // (cfr.rs:421-432, river.rs:264-271) and chance sum (cfr.rs:462-478).
-template <int MODE, int MAXA>
-__global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask* __restrict__ tasks, int chunks) {
-  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
-  const UpTask T = tasks[t];
-  if (A.alive[T.slot] == 0) return;
+template <int MODE, int MAXA, int KIND>
+__device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h0) {
+  const uint32_t live = A.alive[T.slot];
+  if (live == 0) return;
   const int p = A.p;
-  const int hp = A.hp[p];
-  const int h0 = ch * ROW_CHUNK + threadIdx.x * VEC;
+  const int hp = pick(p, A.hp);
   if (h0 >= hp) return;
   const size_t stride = (size_t)A.stride;
   float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (T.kind == U_OWN) {
+  if constexpr (KIND == U_OWN) {
     const int na = (int)T.nchild;
     float4 cfv[MAXA];
+    // Child values and the node's storage block (regrets in CFR, strategy
+    // sums in Average mode) are loaded together.
+    float4 st[MODE == M_BR ? 1 : MAXA];
+    const float* sbase = (MODE == M_CFR ? A.regrets : A.sums) + T.store + h0;
 #pragma unroll
     for (int a = 0; a < MAXA; a++)
       if (a < na) cfv[a] = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
+    if (MODE != M_BR) {
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) st[MODE == M_BR ? 0 : a] = ld4(sbase + (size_t)a * hp);
+    }
     if (MODE == M_BR) {
       out = cfv[0];
 #pragma unroll
@@ -161,12 +180,9 @@ __global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask
 #pragma unroll
           for (int j = 0; j < VEC; j++) at(out, j) = at(cfv[a], j) > at(out, j) ? at(cfv[a], j) : at(out, j);
     } else if (MODE == M_AVG) {
-      float4 s[MAXA];
+      float4* s = st;
       float4 inv;
       const float uniform = 1.0f / (float)na;
-#pragma unroll
-      for (int a = 0; a < MAXA; a++)
-        if (a < na) s[a] = ld4(A.sums + T.store + (size_t)a * hp + h0);
 #pragma unroll
       for (int j = 0; j < VEC; j++) {
         float d = at(s[0], j);
@@ -185,12 +201,9 @@ __global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask
           }
     } else {
       const DiscountD d = *A.disc;
-      float4 r[MAXA];
+      float4* r = st;
       float4 inv;
       float* rb = A.regrets + T.store + h0;
-#pragma unroll
-      for (int a = 0; a < MAXA; a++)
-        if (a < na) r[a] = ld4(rb + (size_t)a * hp);
 #pragma unroll
       for (int j = 0; j < VEC; j++) {
         float s = max0(at(r[0], j));
@@ -226,48 +239,159 @@ __global__ void __launch_bounds__(ROW_THREADS) up_kernel(RowArgs A, const UpTask
           st4(rb + (size_t)a * hp, r[a]);
         }
     }
-  } else if (T.kind == U_OPP_SUM) {
-    for (uint32_t a = 0; a < T.nchild; a++) {
-      if (A.alive[T.child_slot + a] == 0) continue;
-      float4 v = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
+  } else if constexpr (KIND == U_OPP_SUM) {
+    // Loads first (independent), then the sum in child order.
+    const int na = (int)T.nchild;
+    float4 v[MAXA];
+    bool clive[MAXA];
 #pragma unroll
-      for (int j = 0; j < VEC; j++) at(out, j) += at(v, j);
-    }
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) {
+        clive[a] = A.alive[T.child_slot + a] != 0;
+        v[a] = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
+      }
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na && clive[a])
+#pragma unroll
+        for (int j = 0; j < VEC; j++) at(out, j) += at(v[a], j);
   } else {
     double acc[VEC] = {0.0, 0.0, 0.0, 0.0};
-    const uchar4 mc1 = *reinterpret_cast<const uchar4*>(A.hc1[p] + h0);
-    const uchar4 mc2 = *reinterpret_cast<const uchar4*>(A.hc2[p] + h0);
+    const uint8_t* hc1p = pick(p, A.hc1);
+    const uint8_t* hc2p = pick(p, A.hc2);
+    const uchar4 mc1 = *reinterpret_cast<const uchar4*>(hc1p + h0);
+    const uchar4 mc2 = *reinterpret_cast<const uchar4*>(hc2p + h0);
     const uint8_t* cards = A.chance_cards + T.cards;
-    for (uint32_t i = 0; i < T.nchild; i++) {
-      if (A.alive[T.child_slot + i] == 0) continue;
-      const uint8_t card = cards[i];
-      float4 v = ld4(A.vals + (size_t)(T.child + i) * stride + h0);
+    // Children in batches: flags, cards and rows are loaded before the f64
+    // sum, which stays in card order.
+    constexpr int B = 8;
+    for (uint32_t i0 = 0; i0 < T.nchild; i0 += B) {
+      bool live[B];
+      uint8_t card[B];
+      float4 v[B];
 #pragma unroll
-      for (int j = 0; j < VEC; j++) {
-        bool blocked = (&mc1.x)[j] == card || (&mc2.x)[j] == card;
-        acc[j] += blocked ? 0.0 : (double)at(v, j);
+      for (int k = 0; k < B; k++) {
+        const uint32_t i = i0 + k;
+        live[k] = i < T.nchild && A.alive[T.child_slot + i] != 0;
+        card[k] = i < T.nchild ? cards[i] : 255;
       }
-    }
-    for (uint32_t k = 0; k < T.iso_count; k++) {
-      const IsoRefD ref = A.iso[T.iso_first + k];
-      if (A.alive[T.child_slot + ref.ci] == 0) continue;
-      const uint8_t card = cards[ref.ci];
-      const float* row = A.vals + (size_t)(T.child + ref.ci) * stride;
-      const uint16_t* perm = A.perm + (size_t)(p * 6 + ref.pair) * stride;
 #pragma unroll
-      for (int j = 0; j < VEC; j++) {
-        int h = h0 + j;
-        if (h < A.n[p]) {
-          int q = perm[h];
-          bool blocked = A.hc1[p][q] == card || A.hc2[p][q] == card;
-          acc[j] += blocked ? 0.0 : (double)row[q];
+      for (int k = 0; k < B; k++)
+        if (live[k]) v[k] = ld4(A.vals + (size_t)(T.child + i0 + k) * stride + h0);
+#pragma unroll
+      for (int k = 0; k < B; k++)
+        if (live[k])
+#pragma unroll
+          for (int j = 0; j < VEC; j++) {
+            bool blocked = (&mc1.x)[j] == card[k] || (&mc2.x)[j] == card[k];
+            acc[j] += blocked ? 0.0 : (double)at(v[k], j);
+          }
+    }
+    constexpr int BI = 4;
+    const int np = pick(p, A.n);
+    for (uint32_t k0 = 0; k0 < T.iso_count; k0 += BI) {
+      bool live[BI];
+      float x[BI][VEC];
+      bool blk[BI][VEC];
+#pragma unroll
+      for (int k = 0; k < BI; k++) {
+        live[k] = false;
+        if (k0 + k < T.iso_count) {
+          const IsoRefD ref = A.iso[T.iso_first + k0 + k];
+          live[k] = A.alive[T.child_slot + ref.ci] != 0;
+          const uint8_t card = cards[ref.ci];
+          const float* row = A.vals + (size_t)(T.child + ref.ci) * stride;
+          const uint16_t* perm = A.perm + (size_t)(p * 6 + ref.pair) * stride;
+#pragma unroll
+          for (int j = 0; j < VEC; j++) {
+            x[k][j] = 0.0f;
+            blk[k][j] = true;
+            const int h = h0 + j;
+            if (h < np) {
+              const int q = perm[h];
+              blk[k][j] = hc1p[q] == card || hc2p[q] == card;
+              x[k][j] = row[q];
+            }
+          }
         }
       }
+#pragma unroll
+      for (int k = 0; k < BI; k++)
+        if (live[k])
+#pragma unroll
+          for (int j = 0; j < VEC; j++)
+            if (h0 + j < np) acc[j] += blk[k][j] ? 0.0 : (double)x[k][j];
     }
 #pragma unroll
     for (int j = 0; j < VEC; j++) at(out, j) = (float)acc[j];
   }
   st4(A.vals + (size_t)T.node * stride + h0, out);
+}
+
+// ------------------------------------------------------------ level kernels
+// One launch per level, one block per node. Levels are chained with programmatic dependent
+// launch: a level's grid is launched while the previous one drains and waits
+// (griddepcontrol.wait) until that grid has completed and its writes are
+// visible.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_MAX_THREADS) down_kernel(RowArgs A, const DownTask* __restrict__ tasks,
+                                                               int chunks) {
+  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
+  const DownTask T = tasks[t];  // plan data: readable before the wait
+  pdl_wait();
+  const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
+  if (T.kind == D_OPP_SPLIT) down_item<MODE, MAXA, D_OPP_SPLIT>(A, T, h0, threadIdx.x & 31);
+  else down_item<MODE, 1, D_CHANCE_SPLIT>(A, T, h0, threadIdx.x & 31);
+  pdl_launch_dependents();
+}
+
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_MAX_THREADS) up_kernel(RowArgs A, const UpTask* __restrict__ tasks, int chunks) {
+  const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
+  const UpTask T = tasks[t];
+  pdl_wait();
+  const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
+  if (T.kind == U_OWN) up_item<MODE, MAXA, U_OWN>(A, T, h0);
+  else if (T.kind == U_OPP_SUM) up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
+  else up_item<MODE, 1, U_CHANCE_SUM>(A, T, h0);
+  pdl_launch_dependents();
+}
+
+// Fused river subtrees: one block per subtree walks its nodes (see
+// FusedTree). Every thread keeps the same 4 hands throughout, so a node's
+// rows are produced and consumed by the same threads; the barrier between
+// down levels publishes the children's liveness flags.
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_MAX_THREADS) fused_down_kernel(RowArgs A, const FusedTree* __restrict__ trees,
+                                                                     const DownTask* __restrict__ tasks) {
+  const FusedTree F = trees[blockIdx.x];
+  pdl_wait();
+  const int h0 = (int)threadIdx.x * VEC, lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (uint32_t i = 0; i < F.down_count; i++) {
+    const DownTask T = tasks[F.down_first + i];
+    if (T.kind & LEVEL_BREAK) __syncthreads();
+    down_item<MODE, MAXA, D_OPP_SPLIT>(A, T, h0, lane);
+  }
+  pdl_launch_dependents();
+}
+
+template <int MODE, int MAXA>
+__global__ void __launch_bounds__(ROW_MAX_THREADS) fused_up_kernel(RowArgs A, const FusedTree* __restrict__ trees,
+                                                                   const UpTask* __restrict__ tasks) {
+  const FusedTree F = trees[blockIdx.x];
+  pdl_wait();
+  const int h0 = (int)threadIdx.x * VEC;
+#pragma unroll 1
+  for (uint32_t i = 0; i < F.up_count; i++) {
+    const UpTask T = tasks[F.up_first + i];
+    if ((T.kind & KIND_MASK) == U_OWN) up_item<MODE, MAXA, U_OWN>(A, T, h0);
+    else up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
+  }
+  pdl_launch_dependents();
 }
 
 // ------------------------------------------------------------ setup kernels
@@ -443,45 +567,102 @@ __global__ void advance_kernel(uint32_t* counter, const DiscountD* table, uint32
 }
 
 // ---------------------------------------------------------- host launchers
-template <int MODE, int MAXA>
-static void launch_down_t(const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s) {
-  down_kernel<MODE, MAXA><<<ntasks * chunks, ROW_THREADS, 0, s>>>(A, tasks, chunks);
-}
-template <int MODE, int MAXA>
-static void launch_up_t(const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s) {
-  up_kernel<MODE, MAXA><<<ntasks * chunks, ROW_THREADS, 0, s>>>(A, tasks, chunks);
-}
-
-void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int chunks, cudaStream_t s) {
-  if (maxa <= 4) {
-    if (mode == M_CFR) launch_down_t<M_CFR, 4>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_down_t<M_BR, 4>(A, tasks, ntasks, chunks, s);
-    else launch_down_t<M_AVG, 4>(A, tasks, ntasks, chunks, s);
-  } else if (maxa <= 8) {
-    if (mode == M_CFR) launch_down_t<M_CFR, 8>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_down_t<M_BR, 8>(A, tasks, ntasks, chunks, s);
-    else launch_down_t<M_AVG, 8>(A, tasks, ntasks, chunks, s);
-  } else {
-    if (mode == M_CFR) launch_down_t<M_CFR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_down_t<M_BR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
-    else launch_down_t<M_AVG, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
-  }
+// One block per node (and chunk of 4 * ROW_MAX_THREADS hands): a thread per 4
+// hands, whole warps. Launched with programmatic stream serialization so the
+// grid is set up while the previous level drains; the kernel waits
+// (griddepcontrol.wait) before touching rows or storage.
+static int row_threads(int hp) {
+  const int t = ((hp + VEC - 1) / VEC + 31) / 32 * 32;
+  return t < 32 ? 32 : (t > ROW_MAX_THREADS ? ROW_MAX_THREADS : t);
 }
 
-void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int chunks, cudaStream_t s) {
-  if (maxa <= 4) {
-    if (mode == M_CFR) launch_up_t<M_CFR, 4>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_up_t<M_BR, 4>(A, tasks, ntasks, chunks, s);
-    else launch_up_t<M_AVG, 4>(A, tasks, ntasks, chunks, s);
-  } else if (maxa <= 8) {
-    if (mode == M_CFR) launch_up_t<M_CFR, 8>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_up_t<M_BR, 8>(A, tasks, ntasks, chunks, s);
-    else launch_up_t<M_AVG, 8>(A, tasks, ntasks, chunks, s);
-  } else {
-    if (mode == M_CFR) launch_up_t<M_CFR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
-    else if (mode == M_BR) launch_up_t<M_BR, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
-    else launch_up_t<M_AVG, MAX_ACTIONS>(A, tasks, ntasks, chunks, s);
+template <typename K, typename Task>
+static void launch_level(K kernel, const RowArgs& A, const Task* tasks, int ntasks, int hp, cudaStream_t s) {
+  const int threads = row_threads(hp), chunks = (hp + threads * VEC - 1) / (threads * VEC);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ntasks * chunks));
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, A, tasks, chunks);
+}
+
+template <int MODE>
+static void launch_down_m(int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s) {
+  if (maxa <= 4) return launch_level(down_kernel<MODE, 4>, A, tasks, ntasks, hp, s);
+  if (maxa <= 8) return launch_level(down_kernel<MODE, 8>, A, tasks, ntasks, hp, s);
+  launch_level(down_kernel<MODE, MAX_ACTIONS>, A, tasks, ntasks, hp, s);
+}
+
+template <int MODE>
+static void launch_up_m(int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s) {
+  if (maxa <= 4) return launch_level(up_kernel<MODE, 4>, A, tasks, ntasks, hp, s);
+  if (maxa <= 8) return launch_level(up_kernel<MODE, 8>, A, tasks, ntasks, hp, s);
+  launch_level(up_kernel<MODE, MAX_ACTIONS>, A, tasks, ntasks, hp, s);
+}
+
+template <typename K, typename Task>
+static void launch_fused(K kernel, const RowArgs& A, const FusedTree* trees, int ntrees, const Task* tasks, int hp,
+                         cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ntrees);
+  cfg.blockDim = dim3((unsigned)row_threads(hp));
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, A, trees, tasks);
+}
+
+template <int MODE>
+static void launch_fused_m(bool up, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees,
+                           const DownTask* dt, const UpTask* ut, int hp, cudaStream_t s) {
+  if (up) {
+    if (maxa <= 4) return launch_fused(fused_up_kernel<MODE, 4>, A, trees, ntrees, ut, hp, s);
+    if (maxa <= 8) return launch_fused(fused_up_kernel<MODE, 8>, A, trees, ntrees, ut, hp, s);
+    return launch_fused(fused_up_kernel<MODE, MAX_ACTIONS>, A, trees, ntrees, ut, hp, s);
   }
+  if (maxa <= 4) return launch_fused(fused_down_kernel<MODE, 4>, A, trees, ntrees, dt, hp, s);
+  if (maxa <= 8) return launch_fused(fused_down_kernel<MODE, 8>, A, trees, ntrees, dt, hp, s);
+  launch_fused(fused_down_kernel<MODE, MAX_ACTIONS>, A, trees, ntrees, dt, hp, s);
+}
+
+void launch_fused_down(int mode, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees,
+                       const DownTask* tasks, int hp, cudaStream_t s) {
+  if (ntrees <= 0) return;
+  if (mode == M_CFR) launch_fused_m<M_CFR>(false, maxa, A, trees, ntrees, tasks, nullptr, hp, s);
+  else if (mode == M_BR) launch_fused_m<M_BR>(false, maxa, A, trees, ntrees, tasks, nullptr, hp, s);
+  else launch_fused_m<M_AVG>(false, maxa, A, trees, ntrees, tasks, nullptr, hp, s);
+}
+
+void launch_fused_up(int mode, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees, const UpTask* tasks,
+                     int hp, cudaStream_t s) {
+  if (ntrees <= 0) return;
+  if (mode == M_CFR) launch_fused_m<M_CFR>(true, maxa, A, trees, ntrees, nullptr, tasks, hp, s);
+  else if (mode == M_BR) launch_fused_m<M_BR>(true, maxa, A, trees, ntrees, nullptr, tasks, hp, s);
+  else launch_fused_m<M_AVG>(true, maxa, A, trees, ntrees, nullptr, tasks, hp, s);
+}
+
+void launch_down(int mode, int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s) {
+  if (ntasks <= 0) return;
+  if (mode == M_CFR) launch_down_m<M_CFR>(maxa, A, tasks, ntasks, hp, s);
+  else if (mode == M_BR) launch_down_m<M_BR>(maxa, A, tasks, ntasks, hp, s);
+  else launch_down_m<M_AVG>(maxa, A, tasks, ntasks, hp, s);
+}
+
+void launch_up(int mode, int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s) {
+  if (ntasks <= 0) return;
+  if (mode == M_CFR) launch_up_m<M_CFR>(maxa, A, tasks, ntasks, hp, s);
+  else if (mode == M_BR) launch_up_m<M_BR>(maxa, A, tasks, ntasks, hp, s);
+  else launch_up_m<M_AVG>(maxa, A, tasks, ntasks, hp, s);
 }
 
 void launch_strength(const uint8_t* boards, int nboards, const uint8_t* hc1_0, const uint8_t* hc2_0,

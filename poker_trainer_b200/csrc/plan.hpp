@@ -19,8 +19,7 @@
 namespace dcfr {
 
 constexpr int VEC = 4;             // hands per thread in the row kernels (float4)
-constexpr int ROW_THREADS = 128;   // threads per row-kernel block
-constexpr int ROW_CHUNK = VEC * ROW_THREADS;
+constexpr int ROW_MAX_THREADS = 352;  // row-kernel block: a thread per 4 hands, whole warps (1328 hands max)
 constexpr int MAX_ACTIONS = 16;
 constexpr int TERM_WARPS = 4;      // warps per terminal-kernel block
 constexpr int TERM_CHUNK = 32;     // sweep steps staged per cp.async batch
@@ -54,6 +53,16 @@ struct UpTask {
   uint32_t iso_count;
   uint32_t pad;
 };
+
+// Fused river subtree: the down and up tasks of all its decision nodes,
+// processed by one block (down: BFS order, LEVEL_BREAK on a level's first
+// task; up: deepest level first).
+struct FusedTree {
+  uint32_t down_first, down_count;
+  uint32_t up_first, up_count;
+};
+constexpr uint32_t LEVEL_BREAK = 0x100u;  // in DownTask::kind
+constexpr uint32_t KIND_MASK = 0xFFu;
 
 struct IsoRefD {
   uint16_t ci;    // canonical child index

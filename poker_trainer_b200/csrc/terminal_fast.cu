@@ -115,55 +115,144 @@ __global__ void fast_layout_kernel(const EntryD* __restrict__ tables, const uint
   }
 }
 
-// One block per task at a time (grid-stride over the task list).
+// Shared-memory layout of a block (all offsets 16-byte aligned).
+struct FastSmem {
+  size_t rbuf, r64, g, cs, wsum, fred, cat, rec, same, seg, total;
+  __host__ __device__ FastSmem(int stride, int emax, int cstride, int tstride) {
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t gn = (size_t)FAST_THREADS * emax + 2;
+    rbuf = 0;
+    r64 = up16(rbuf + 2 * (size_t)stride * 4);
+    g = up16(r64 + ((size_t)stride + 1) * 8);
+    cs = up16(g + gn * 8);
+    wsum = up16(cs + 2 * FAST_SEGS * 8);
+    fred = up16(wsum + (FAST_THREADS / 32) * 8);
+    cat = up16(fred + 2 * (FAST_THREADS / 32) * 4);
+    rec = up16(cat + (size_t)cstride * 2);
+    same = up16(rec + (size_t)tstride * 16);
+    seg = up16(same + (size_t)stride * 2);
+    total = up16(seg + FAST_SEGS * 2);
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Each block takes a contiguous range of the (board-sorted) task list. The
+// board's layout (elements, segment starts, per-hand records) is staged in
+// shared memory when the board changes, and the next task's reach row is
+// copied in (cp.async) while the current one is evaluated. E (elements per
+// thread of the scan, odd) is a compile-time constant so a thread's elements
+// stay in registers between the two passes of the scan.
+template <int E>
 __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A, const FastTask* __restrict__ tasks,
                                                                      int ntasks) {
   extern __shared__ __align__(16) unsigned char smem_fast[];
-  const int E = A.emax;
-  const int gn = (FAST_THREADS * E + 2) & ~1;
-  float* r = reinterpret_cast<float*>(smem_fast);
-  long long* G = reinterpret_cast<long long*>(r + A.stride);
-  long long* Cs = G + gn;
-  long long* wsum = Cs + FAST_SEGS;
-  float* fred = reinterpret_cast<float*>(wsum + FAST_THREADS / 32);
+  const FastSmem L_(A.stride, E, A.cstride, A.tstride);
+  float* rbuf = reinterpret_cast<float*>(smem_fast + L_.rbuf);
+  long long* R64 = reinterpret_cast<long long*>(smem_fast + L_.r64);
+  long long* G = reinterpret_cast<long long*>(smem_fast + L_.g);
+  longlong2* Cs = reinterpret_cast<longlong2*>(smem_fast + L_.cs);  // per card: {start prefix, card total}
+  long long* wsum = reinterpret_cast<long long*>(smem_fast + L_.wsum);
+  float* fred = reinterpret_cast<float*>(smem_fast + L_.fred);
+  uint16_t* scat = reinterpret_cast<uint16_t*>(smem_fast + L_.cat);
+  uint4* srec = reinterpret_cast<uint4*>(smem_fast + L_.rec);
+  uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_fast + L_.same);
+  uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_fast + L_.seg);
 
   const int p = A.p, o = p ^ 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
-  for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
-    const FastTask& T = tasks[ti];
-    const uint32_t slot = T.slot;
-    if (A.alive[slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
-    const size_t lay = (size_t)T.board * 2 + p;
-    const uint16_t* seg = A.seg + lay * FAST_SEGS;
-    const int L = seg[FAST_SEGS - 1];
+  const int per = (ntasks + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(ntasks, t0 + per);
+  if (t0 >= t1) return;
 
-    // Reach row into shared memory, and its maximum.
-    const float4* src = reinterpret_cast<const float4*>(A.reach + (size_t)slot * A.stride);
+  for (int h = tid; h < hpp; h += FAST_THREADS) {
+    const uint32_t sm = h < np ? A.same[h] : NONE32;
+    ssame[h] = sm == NONE32 ? (uint16_t)hpo : (uint16_t)sm;  // R64[hpo] is zero
+  }
+  if (tid == 0) R64[hpo] = 0;
+  auto prefetch = [&](int ti, int buf) {
+    const float* src = A.reach + (size_t)tasks[ti].slot * A.stride;
+    float* dst = rbuf + (size_t)buf * A.stride;
+    for (int i = tid; i < hpo / 4; i += FAST_THREADS) cp_async16(dst + 4 * i, src + 4 * i);
+    cp_async_commit();
+  };
+  prefetch(t0, 0);
+  uint32_t board = NONE32;
+  int L = 0;
+
+  for (int ti = t0; ti < t1; ti++) {
+    const int buf = (ti - t0) & 1;
+    const float* r = rbuf + (size_t)buf * A.stride;
+    // Row ti landed (own copies), partial maxima published.
+    cp_async_wait_all();
     float mx = 0.0f;
     for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
-      const float4 v = src[i];
-      reinterpret_cast<float4*>(r)[i] = v;
+      const float4 v = reinterpret_cast<const float4*>(r)[i];
       mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-    if (lane == 0) fred[warp] = mx;
+    if (lane == 0) fred[buf * (FAST_THREADS / 32) + warp] = mx;
     __syncthreads();
+    if (ti + 1 < t1) prefetch(ti + 1, buf ^ 1);
+
+    const FastTask* T = tasks + ti;
+    const uint32_t slot = T->slot, tb = T->board, row = T->row, frow = T->frow, kind = T->kind;
+    const double pa0 = T->a, pb0 = T->b, pc0 = T->c, pd0 = T->d;
+    if (A.alive[slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
+    const size_t lay = (size_t)tb * 2 + p;
+    if (tb != board) {
+      board = tb;
+      const uint16_t* gseg = A.seg + lay * FAST_SEGS;
+      if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
+      L = gseg[FAST_SEGS - 1];
+      const uint16_t* gcat = A.cat + lay * A.cstride;
+      for (int k = tid; k < L; k += FAST_THREADS) scat[k] = gcat[k];
+      const uint4* grec = A.rec + lay * A.tstride;
+      for (int h = tid; h < np; h += FAST_THREADS) srec[h] = grec[h];
+    }
+    mx = 0.0f;
 #pragma unroll
-    for (int w = 0; w < FAST_THREADS / 32; w++) mx = fmaxf(mx, fred[w]);
+    for (int w = 0; w < FAST_THREADS / 32; w++) mx = fmaxf(mx, fred[buf * (FAST_THREADS / 32) + w]);
     // Row sum < 2048 * 2^(e+1) with 2^e <= max: scale it below 2^62.
     const int S = 177 - (int)((__float_as_uint(mx) >> 23) & 0xFF);
     const double scale = pow2(S), inv = pow2(-S);
+    // Payoffs times 2^-S (exact: a power-of-two scaling).
+    const double pa = pa0 * inv, pb = pb0 * inv, pc = pc0 * inv, pd = pd0 * inv;
 
-    // Elements in layout order, as fixed point.
-    const uint16_t* cat = A.cat + lay * A.cstride;
-    for (int k = tid; k < FAST_THREADS * E; k += FAST_THREADS) G[k] = k < L ? fixed(r[cat[k]], scale) : 0;
+    // Reach row as fixed point.
+    for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
+      const float4 v = reinterpret_cast<const float4*>(r)[i];
+      R64[4 * i + 0] = fixed(v.x, scale);
+      R64[4 * i + 1] = fixed(v.y, scale);
+      R64[4 * i + 2] = fixed(v.z, scale);
+      R64[4 * i + 3] = fixed(v.w, scale);
+    }
+    __syncthreads();
+
+    // Elements in layout order.
+    constexpr int N = FAST_THREADS * E;
+#pragma unroll
+    for (int u = 0; u < E; u++) {
+      const int k = tid + u * FAST_THREADS;
+      G[k] = R64[k < L ? (int)scat[k] : hpo];
+    }
     __syncthreads();
 
     // Exclusive prefix sums, in place: E consecutive elements per thread.
     long long* own = G + tid * E;
+    long long x[E];
     long long local = 0;
-    for (int i = 0; i < E; i++) local += own[i];
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+      x[i] = own[i];
+      local += x[i];
+    }
     long long inc = local;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -173,86 +262,106 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
     if (lane == 31) wsum[warp] = inc;
     __syncthreads();
     long long acc = inc - local;
-    for (int w = 0; w < warp; w++) acc += wsum[w];
+#pragma unroll
+    for (int w = 0; w < FAST_THREADS / 32; w++)
+      if (w < warp) acc += wsum[w];
+#pragma unroll
     for (int i = 0; i < E; i++) {
-      const long long x = own[i];
       own[i] = acc;
-      acc += x;
+      acc += x[i];
     }
-    if (tid == FAST_THREADS - 1) G[FAST_THREADS * E] = acc;
+    if (tid == FAST_THREADS - 1) G[N] = acc;
     __syncthreads();
-    if (tid < FAST_SEGS) Cs[tid] = G[seg[tid]];
+    if (tid < FAST_SEGS - 1) {
+      const long long c0 = G[sseg[tid]], c1 = G[sseg[tid + 1]];
+      Cs[tid] = make_longlong2(c0, c1 - c0);
+    }
     __syncthreads();
 
-    // Values in hand order.
-    const uint4* rec = A.rec + lay * A.tstride;
-    const long long T0 = Cs[1];
-    float* out = A.vals + (size_t)T.row * A.stride;
-    const uint32_t frow = T.frow, kind = T.kind;
+    // Values in hand order. Cs[0] = {0, T0}; Cs[1 + c] = card c.
+    const long long T0 = Cs[0].y;
+    float* out = A.vals + (size_t)row * A.stride;
     float* fout = frow != NONE32 ? A.vals + (size_t)frow * A.stride : nullptr;
     const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
     const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
-    const double pa = T.a, pb = T.b, pc = T.c, pd = T.d;
+#pragma unroll 2
     for (int h = tid; h < hpp; h += FAST_THREADS) {
       float v = 0.0f, fv = 0.0f;
       if (h < np) {
-        const uint4 q = rec[h];
-        const int a = q.w & 0xFF, b = (q.w >> 8) & 0xFF;
-        const long long C0a = Cs[1 + a], CTa = Cs[2 + a] - C0a;
-        const long long C0b = Cs[1 + b], CTb = Cs[2 + b] - C0b;
-        const uint32_t sm = A.same[h];
-        const long long si = sm != NONE32 ? fixed(r[sm], scale) : 0;
-        const long long F = T0 - CTa - CTb + si;
+        const uint4 q = srec[h];
+        const longlong2 ca = Cs[1 + (q.w & 0xFF)], cb = Cs[1 + ((q.w >> 8) & 0xFF)];
+        const long long si = R64[ssame[h]];
+        const long long F = T0 - ca.y - cb.y + si;
         if (fold) {
           // eval_fold (eval.rs:40-64) returns zeros on a zero total.
-          v = (scalar && T0 == 0) ? 0.0f : (float)(pa * ((double)F * inv));
+          v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
         } else {
           if (q.w >> 16) {
             const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
-            const long long Ca = G[q.y & 0xFFFF] - C0a, Cal = G[q.y >> 16] - C0a;
-            const long long Cb = G[q.z & 0xFFFF] - C0b, Cbl = G[q.z >> 16] - C0b;
-            const double fw = (double)(Gw - Ca - Cb) * inv;
-            const double fl = (double)((T0 - Gs) - (CTa - Cal) - (CTb - Cbl)) * inv;
+            const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
+            const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
+            // weaker: Gw - (Gaw - C0a) - (Gbw - C0b); stronger: (T0 - Gs)
+            // - (CTa - (Gas - C0a)) - (CTb - (Gbs - C0b)).
+            const long long W = (Gw + ca.x + cb.x) - Gaw - Gbw;
+            const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
             if (scalar) {
-              v = (float)(pa * fw) + (float)(pb * fl);
+              v = (float)(pa * (double)W) + (float)(pb * (double)Lx);
             } else {
-              double res = pa * fw;
-              res += pb * fl;
+              double res = pa * (double)W;
+              res += pb * (double)Lx;
               v = (float)res;
             }
-            if (pc != 0.0) {
-              const long long eq = (Gs - Gw) - (Cal - Ca) - (Cbl - Cb) + si;
-              v += (float)(pc * ((double)eq * inv));
+            if (pc0 != 0.0) {
+              const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+              v += (float)(pc * (double)eq);
             }
           }
-          fv = (float)(pd * ((double)F * inv));
+          if (fout) fv = (float)(pd * (double)F);
         }
       }
       out[h] = v;
       if (fout) fout[h] = fv;
     }
-    __syncthreads();
   }
+  cp_async_wait_all();
+}
+
+template <int E>
+static cudaError_t setup_e(int optin, size_t smem, int& blocks) {
+  cudaError_t e = cudaFuncSetAttribute(fast_terminal_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel<E>, FAST_THREADS, smem);
 }
 
 int fast_emax(int tstride) {
   const int e = (3 * tstride + FAST_THREADS - 1) / FAST_THREADS;
-  return e | 1;  // odd: conflict-free strided f64 access
+  return e | 1;  // odd: conflict-free strided 8-byte access
 }
 
-size_t fast_smem_bytes(int stride, int emax) {
-  const int gn = (FAST_THREADS * emax + 2) & ~1;
-  return (size_t)stride * 4 + (size_t)gn * 8 + FAST_SEGS * 8 + (FAST_THREADS / 32) * 8 + (FAST_THREADS / 32) * 4;
+size_t fast_smem_bytes(int stride, int emax, int cstride, int tstride) {
+  return FastSmem(stride, emax, cstride, tstride).total;
 }
 
-int fast_blocks_per_sm(int stride, int emax) {
+int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride) {
   int blocks = 0;
-  const size_t smem = fast_smem_bytes(stride, emax);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(fast_terminal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel, FAST_THREADS, smem) != cudaSuccess)
-    return 1;
-  return blocks > 0 ? blocks : 1;
+  const size_t smem = fast_smem_bytes(stride, emax, cstride, tstride);
+  // The limit is the device's opt-in maximum (a per-kernel setting shared by
+  // every handle), not this handle's size.
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  if ((size_t)optin < smem) return 0;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (emax) {
+#define FAST_E(e_)                          \
+  case e_:                                  \
+    e = setup_e<e_>(optin, smem, blocks);   \
+    break;
+    FAST_E(1) FAST_E(3) FAST_E(5) FAST_E(7) FAST_E(9) FAST_E(11) FAST_E(13) FAST_E(15) FAST_E(17)
+#undef FAST_E
+  }
+  return e == cudaSuccess ? blocks : 0;
 }
 
 void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstride, int nboards, const uint8_t* hc1_0,
@@ -266,7 +375,15 @@ void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstrid
 void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s) {
   if (ntasks <= 0) return;
   const int blocks = ntasks < max_blocks ? ntasks : max_blocks;
-  fast_terminal_kernel<<<blocks, FAST_THREADS, fast_smem_bytes(A.stride, A.emax), s>>>(A, tasks, ntasks);
+  const size_t smem = fast_smem_bytes(A.stride, A.emax, A.cstride, A.tstride);
+  switch (A.emax) {
+#define FAST_E(e_)                                                                  \
+  case e_:                                                                          \
+    fast_terminal_kernel<e_><<<blocks, FAST_THREADS, smem, s>>>(A, tasks, ntasks); \
+    break;
+    FAST_E(1) FAST_E(3) FAST_E(5) FAST_E(7) FAST_E(9) FAST_E(11) FAST_E(13) FAST_E(15) FAST_E(17)
+#undef FAST_E
+  }
 }
 
 }  // namespace dcfr
