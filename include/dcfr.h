@@ -321,6 +321,30 @@ typedef struct dcfr_kernel_profile {
  * every class boundary, and returns the per-class totals. */
 int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profile* out);
 
+/* Largest hand count per side that dcfr_showdown_values_noalloc accepts. */
+#define DCFR_NOALLOC_MAX_HANDS 1326
+
+/* No counterpart in the reference: range-vs-range showdown values on one
+ * river board, for callers that cannot allocate device memory (a host whose
+ * device memory belongs to its own pool allocator, or work enqueued while a
+ * stream is being captured, where cudaMalloc is not allowed). It allocates
+ * nothing: its scratch is one static device array of 192 KiB that every GPU
+ * loading the library holds until exit. For each hero hand h,
+ *   out[h] = win  * (sum of opp_reach over opponent hands weaker than h)
+ *          + lose * (sum over stronger hands) + tie * (sum over equal hands),
+ * counting only opponent hands that share no card with h (lose is signed:
+ * pass a negative payoff). board (5 cards) and the two hand lists (2 card
+ * ids per hand, no board cards, no repeats, at most DCFR_NOALLOC_MAX_HANDS
+ * each) are host memory; opp_reach (n_opp floats) and out (n_hero floats)
+ * are device memory; stream is a cudaStream_t (NULL: the default stream) and
+ * the call is asynchronous on it. Calls share the scratch array: calls whose
+ * work overlaps on the GPU race and must be serialised by the caller. The
+ * first call on each device does a one-time set-up with that device current;
+ * make it before any stream capture. */
+int dcfr_showdown_values_noalloc(const uint8_t board[5], const uint8_t* hero_cards, int32_t n_hero,
+                                 const uint8_t* opp_cards, int32_t n_opp, const float* opp_reach, double win,
+                                 double lose, double tie, float* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,11 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+namespace dcfr {
+// Lets the library's other translation units report through dcfr_last_error.
+void set_last_error(const std::string& msg) { g_error = msg; }
+}  // namespace dcfr
+
 static int done(const dcfr::Status& s) {
   if (s.ok()) {
     g_error.clear();

@@ -29,6 +29,7 @@ EXPORTS = [
     "dcfr_actions_at", "dcfr_query_sizes", "dcfr_query", "dcfr_ranges_after", "dcfr_storage_len",
     "dcfr_download_storage", "dcfr_upload_storage", "dcfr_set_iterations", "dcfr_traverse",
     "dcfr_kernel_launches", "dcfr_last_iterate_ms", "dcfr_iteration_bytes", "dcfr_iterate_profiled",
+    "dcfr_showdown_values_noalloc",
 ]
 
 
