@@ -49,12 +49,20 @@ WORKLOADS = {
              "DCFR alpha 1.5 beta 0 gamma 2"),
     "river": ("river subgame Ks7s2dTh4c: pot 20bb, stacks 90bb, bets 50%/100%/all-in + 2.5x raise, seeded class "
               "ranges (seeds 1000/1001), f32 storage, DCFR alpha 1.5 beta 0 gamma 2"),
+    "batch": ("512 independent river spots in one persistent launch per block of iterations under a captured CUDA "
+              "graph: 5-card boards from seed 3000, pots U[400,6000] chips, stacks U[2000,15000], menus of 1-3 sizes from "
+              "{33,50,75,100,150}% plus all-in for bets and raises, trees of 15-400 nodes, seeded class ranges, f32, "
+              "DCFR alpha 1.5 beta 0 gamma 2, 500 iterations each, autotuned launch shape"),
+    "flop": ("flop full tree Ks7s2d: pot 6bb, stacks 97bb, bets 33%/75%/all-in + 3x raise on every street, "
+             "Dirichlet(0.5) class ranges thresholded to 68 of 169 classes (seeds 2000/2001), f32 storage, "
+             "suit isomorphism, DCFR alpha 1.5 beta 0 gamma 2; solved to 0.5% of the pot"),
 }
 
 
 def workload_config(name: str, precision: str):
     from poker_trainer_b200 import workloads
-    cfg = workloads.turn_spot() if name == "turn" else workloads.river_spot()
+    cfg = {"turn": workloads.turn_spot, "river": workloads.river_spot, "flop": workloads.flop_spot,
+           "batch": workloads.river_spot}[name]()
     from poker_trainer_b200 import abi
     cfg.precision = abi.PRECISIONS[precision]
     return cfg
@@ -190,6 +198,9 @@ def ncu_traffic(kernel: str, workload: str):
 
 
 KERNEL_NAMES = {"terminal": "fast_terminal_kernel", "down": "down_kernel", "up": "up_kernel", "other": "other"}
+# The terminal kernel the engine picks by hand count (more than 768 hands:
+# one block-wide scan per terminal; otherwise one warp per terminal).
+TERMINAL_KERNEL = {"turn": "fast_terminal_kernel", "river": "fast_terminal_kernel", "flop": "warp_terminal_kernel"}
 
 
 def dist_setup(n_gpus: int):
@@ -328,6 +339,9 @@ def run_ours(args, world, rank, local):
                          f"host threads (C++ restatement of the reference's CPU solver)"}
 
     working = it_bytes
+    kname = KERNEL_NAMES[dom]
+    if dom == "terminal":
+        kname = TERMINAL_KERNEL[args.workload] if args.precision == "fast" else "terminal_kernel"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -347,10 +361,9 @@ def run_ours(args, world, rank, local):
                 "what": "dcfr_create from the host config + K iterations + regrets and sums read back into pinned "
                         "host memory, wall clock, max over ranks; bytes are the per-solve totals / K"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom] if args.precision == "fast" or dom != "terminal"
-                     else "terminal_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
-                     "traffic": ncu_traffic(KERNEL_NAMES[dom], args.workload),
+                     "traffic": ncu_traffic(kname, args.workload),
                      "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms},
         "iteration_roofline": {"bytes_per_iteration": it_bytes,
                                "achieved": it_bytes * (K / (ms / 1000.0)) / 1e9, "peak": peak, "unit": "GB/s",
@@ -367,6 +380,217 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_flop(args, world, rank, local):
+    """Time to 0.5%-of-pot exploitability on the flop workload: dcfr_solve from
+    a fresh solver with exploitability checks on the reference's schedule
+    (check every 10 iterations, then aimed at the predicted iteration), the
+    final exploitability re-checked by the FP64 best-response oracle; then K
+    profiled iterations for the roofline. The CPU figure is the oracle's
+    time per iteration on a bounded sample times the same iteration count
+    (the algorithm and its iteration count are the same on both sides), plus
+    one best-response pass per check."""
+    import torch
+    from poker_trainer_b200.solver import Solver, SolveOptions
+
+    torch.cuda.set_device(local)
+    cfg = workload_config("flop", args.precision)
+    pot = float(cfg.root.pot)
+    t0 = time.perf_counter()
+    g = Solver.new(cfg)
+    t_create = time.perf_counter() - t0
+    checks = []
+    sampler = ClockSampler(local) if rank == 0 else None
+    time.sleep(0.5)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.begin()
+    t0 = time.perf_counter()
+    prog = g.solve(SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10),
+                   on_progress=lambda pr: checks.append((pr.iteration, pr.exploitability_pct)) or True)
+    g.synchronize()
+    t_solve = time.perf_counter() - t0
+    if sampler:
+        sampler.end()
+    clocks = sampler.close() if sampler else None
+    e32 = g.exploitability()
+    e64, _ = g.exploitability_fp64()
+    K = args.steps
+    prof = g.iterate_profiled(K)
+    it_bytes = g.iteration_bytes()
+    g.close()
+    ms = prof["total_ms"]
+    peak, peak_kind = measured_peak()
+    classes = prof["classes"]
+    kernels = {c: {"launches": v["launches"], "ms": v["ms"], "share": v["ms"] / max(ms, 1e-12),
+                   "gbs": (v["bytes"] / (v["ms"] / 1000.0) / 1e9) if v["ms"] > 0 else None}
+               for c, v in classes.items()}
+    dom = max(("down", "terminal", "up"), key=lambda c: classes[c]["ms"])
+    dc = classes[dom]
+    per_launch_ms = dc["ms"] / max(dc["launches"], 1)
+    per_launch_bytes = dc["bytes"] / max(dc["launches"], 1)
+    achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
+    kname = TERMINAL_KERNEL["flop"] if dom == "terminal" else KERNEL_NAMES[dom]
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        steps, secs, used = time_oracle(cfg, threads, 1, args.cpu_flop_iters, None)
+        per_it = secs / steps
+        # A check is two best-response traversals: about one iteration.
+        cpu_ttt = per_it * (prog.iteration + len(checks))
+        cpu = {"value": 1.0 / per_it, "unit": UNIT, "cores": used, "kind": "port",
+               "sample": f"{steps} DCFR iterations of the flop workload after 1 untimed, {secs:.1f} s on {used} host "
+                         f"threads (C++ restatement of the reference's CPU solver)",
+               "time_to_target_s": cpu_ttt,
+               "time_to_target_basis": f"{per_it:.3f} s/iteration x ({prog.iteration} iterations + "
+                                       f"{len(checks)} checks)"}
+    line = {
+        "metric": METRIC, "value": K / (ms / 1000.0), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOADS["flop"], "precision": args.precision, "parallelism": "single GPU",
+                   "l2": f"inputs larger than L2: one iteration moves {it_bytes / 1e9:.1f} GB"},
+        "time_to_target": {"seconds": t_solve, "iterations": prog.iteration, "checks": len(checks),
+                           "exploitability_pct": prog.exploitability_pct, "target_pct": 0.5,
+                           "create_seconds": t_create,
+                           "fp64_oracle_exploitability_pct": 100.0 * e64 / pot,
+                           "f32_exploitability_pct": 100.0 * e32 / pot,
+                           "fp64_vs_f32_rel": abs(e64 - e32) / max(abs(e64), 1e-30),
+                           "speedup_vs_cpu": (cpu["time_to_target_s"] / t_solve) if cpu else None},
+        "checks": checks,
+        "clocks": clocks,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
+                     "traffic": ncu_traffic(kname, "flop"), "bytes_per_launch": per_launch_bytes,
+                     "ms_per_launch": per_launch_ms},
+        "iteration_roofline": {"bytes_per_iteration": it_bytes,
+                               "achieved": it_bytes * (K / (ms / 1000.0)) / 1e9, "peak": peak, "unit": "GB/s",
+                               "frac": it_bytes * (K / (ms / 1000.0)) / 1e9 / peak},
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch_configs():
+    from poker_trainer_b200 import workloads
+    from poker_trainer_b200.solver import Solver
+
+    def nodes(c):
+        st = Solver.estimate(c)
+        return st.player_nodes + st.chance_nodes + st.terminal_nodes
+    return workloads.batched_river_spots(count=512, seed=3000, estimate=nodes)
+
+
+def run_batch(args, world, rank, local):
+    """The batched river workload: every rank solves its own copy of the 512
+    spots (replicas); a step is one DCFR iteration of every spot, reported
+    as spot-iterations per second."""
+    import numpy as np
+    import torch
+    from poker_trainer_b200.solver import BatchSolver
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=dt.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+
+    def reduce_max(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    cfgs = batch_configs()
+    S = len(cfgs)
+    K, W = args.steps, args.warmup
+    # End to end: create from host configs, K iterations, storage of every spot read back.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e = BatchSolver.new(cfgs)
+    tuned = e2e.autotune(10)
+    e2e.iterate(K)
+    d2h = 0
+    for i in range(S):
+        r, sm = e2e.download_storage(i)
+        d2h += r.nbytes + sm.nbytes
+    t_e2e = reduce_max(time.perf_counter() - t0)
+    e2e.close()
+    b = BatchSolver.new(cfgs)
+    b.set_tuning(tuned)
+    b.iterate(W)
+    sampler = ClockSampler(local) if rank == 0 else None
+    time.sleep(0.5)
+    l0 = b.kernel_launches()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.begin()
+    b.iterate(K)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.end()
+    clocks = sampler.close() if sampler else None
+    ms = reduce_max(b.last_iterate_ms())
+    launches = b.kernel_launches() - l0
+    expl = b.exploitability()
+    pots = np.array([c.root.pot for c in cfgs], np.float64)
+    it_bytes = b.iteration_bytes()
+    b.close()
+    value = world * S * K / (ms / 1000.0)
+    peak, peak_kind = measured_peak()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline and rank == 0:
+        L = oracle_lib()
+        L.oracle_batch_iterate.argtypes = [C.c_void_p, C.c_int, C.c_uint32, C.c_int]
+        threads = os.cpu_count() or 1
+        L.oracle_set_threads(1)
+        err = C.c_int(0)
+        hs = [L.oracle_create(C.byref(c), C.byref(err)) for c in cfgs]
+        arr = (C.c_void_p * S)(*hs)
+        L.oracle_batch_iterate(arr, S, 1, threads)
+        n_cpu = args.cpu_batch_iters
+        tc0 = time.perf_counter()
+        L.oracle_batch_iterate(arr, S, n_cpu, threads)
+        secs = time.perf_counter() - tc0
+        for h in hs:
+            L.oracle_destroy(h)
+        cpu = {"value": S * n_cpu / secs, "unit": "spot-iterations/s", "cores": threads, "kind": "port",
+               "sample": f"{n_cpu} DCFR iterations of each of the {S} spots after 1 untimed, {secs:.1f} s, spots spread "
+                         f"over {threads} host threads (C++ restatement of the reference's CPU solver)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "spot-iterations/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS["batch"], "spots": S, "iterations_per_step": 1,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tuning": {"warps": tuned.warps, "blocks_per_sm": tuned.blocks_per_sm,
+                              "iterations_per_launch": tuned.iterations_per_launch,
+                              "longest_first": tuned.longest_first, "candidates": tuned.candidates},
+                   "l2": f"one iteration of all spots moves {it_bytes / 1e9:.2f} GB (> 126 MB L2), no flush"},
+        "solve_ms": ms, "clocks": clocks,
+        "e2e": {"value": world * S * K / t_e2e, "unit": "spot-iterations/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h / K,
+                "what": "dcfr_batch_create + autotune + K iterations + every spot's storage read back, wall clock"},
+        "gpu_launches": int(launches),
+        "iteration_roofline": {"bytes_per_iteration": it_bytes, "achieved": it_bytes * K / (ms / 1000.0) / 1e9,
+                               "peak": peak, "unit": "GB/s", "frac": it_bytes * K / (ms / 1000.0) / 1e9 / peak,
+                               "peak_kind": f"of {peak_kind}"},
+        "exploitability_pct_mean_after": float(np.mean(100.0 * expl / pots)),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -378,12 +602,19 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-iterations", type=int, default=2000, help="flop: iteration cap of the timed solve")
+    ap.add_argument("--cpu-flop-iters", type=int, default=3, help="flop: oracle iterations timed for the CPU figure")
+    ap.add_argument("--cpu-batch-iters", type=int, default=20, help="batch: oracle iterations per spot timed")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload == "flop":
+        return run_flop(args, world, rank, local)
+    if args.workload == "batch":
+        return run_batch(args, world, rank, local)
     return run_ours(args, world, rank, local)
 
 

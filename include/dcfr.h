@@ -246,6 +246,14 @@ int dcfr_synchronize(dcfr_solver* s);
 
 /* Solver::exploitability (lib.rs:462-464), chips. */
 int dcfr_exploitability(dcfr_solver* s, double* out);
+/* No counterpart in the reference: the FP64 best-response oracle. The same
+ * exploitability as dcfr_exploitability (cfr.rs:482-502), with every reach
+ * and value row of the two best-response traversals held in double on the
+ * GPU (average strategies normalised in double from the f32 sums, terminal
+ * sums exact in 64-bit fixed point, payoffs in double). best_response (may be
+ * NULL) receives each player's best-response root value in chips. The first
+ * call allocates the double rows on the device. */
+int dcfr_exploitability_fp64(dcfr_solver* s, double* out, double best_response[2]);
 /* Solver::root_values (lib.rs:468-470): average-strategy EV of each player. */
 int dcfr_root_values(dcfr_solver* s, double out[2]);
 /* Solver::iterations, last_exploitability, stats, root_pot. */
@@ -320,6 +328,80 @@ typedef struct dcfr_kernel_profile {
  * captured graph that also records a CUDA event on the handle's stream at
  * every class boundary, and returns the per-class totals. */
 int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profile* out);
+
+/* ---- Batched river solves (no counterpart in the reference) ----------
+ * Many independent river spots (5-card board, river root, fast precision,
+ * one shared DcfrParams) solved together: each DCFR iteration of every spot
+ * is the same as a single dcfr_create/dcfr_iterate solve of that spot, done
+ * by one persistent kernel per block of iterations launched from a captured
+ * CUDA graph; spots of uneven tree size are taken from a work counter,
+ * longest first. */
+typedef struct dcfr_batch dcfr_batch;
+
+/* Launch shape of the batched kernel, chosen by dcfr_batch_autotune. */
+typedef struct dcfr_batch_tuning {
+  int32_t warps;                  /* warps per block (each evaluates terminals) */
+  int32_t blocks_per_sm;          /* resident blocks per SM (grid = SMs x this) */
+  uint32_t iterations_per_launch; /* iterations of a spot per persistent launch */
+  int32_t longest_first;          /* 1: spots taken by decreasing work; 0: input order */
+  int32_t candidates;             /* autotune: candidates timed */
+  int32_t _pad;
+  double trial_ms;                /* autotune: the best candidate's time */
+} dcfr_batch_tuning;
+
+int dcfr_batch_create(const dcfr_config* cfgs, int32_t count, dcfr_batch** out);
+void dcfr_batch_destroy(dcfr_batch* b);
+/* n DCFR iterations of every spot (cpu_iteration, lib.rs:577-585, per spot). */
+int dcfr_batch_iterate(dcfr_batch* b, uint32_t n);
+/* Per-spot exploitability in chips (cfr.rs:482-502); out has count entries. */
+int dcfr_batch_exploitability(dcfr_batch* b, double* out);
+/* One spot's storage in the reference layout (as dcfr_download_storage). */
+int dcfr_batch_storage_len(const dcfr_batch* b, int32_t spot, uint64_t* len);
+int dcfr_batch_download_storage(dcfr_batch* b, int32_t spot, float* regrets, float* sums, uint64_t len);
+/* Times every launch shape that fits on trial_iterations iterations from a
+ * snapshot of the storage (restored after each trial) and keeps the fastest. */
+int dcfr_batch_autotune(dcfr_batch* b, uint32_t trial_iterations, dcfr_batch_tuning* out);
+int dcfr_batch_get_tuning(const dcfr_batch* b, dcfr_batch_tuning* out);
+int dcfr_batch_set_tuning(dcfr_batch* b, const dcfr_batch_tuning* t);
+/* Device time of the last dcfr_batch_iterate (CUDA events on its stream),
+ * iterations done, and kernel launches issued. */
+int dcfr_batch_last_iterate_ms(const dcfr_batch* b, double* ms);
+int dcfr_batch_iterations(const dcfr_batch* b, uint32_t* out);
+int dcfr_batch_kernel_launches(const dcfr_batch* b, uint64_t* out);
+/* Algorithmic bytes of one iteration of every spot (as dcfr_iteration_bytes,
+ * summed over spots). */
+int dcfr_batch_iteration_bytes(const dcfr_batch* b, double* bytes);
+
+/* ---- Leaf-value network (no counterpart in the reference) ---------------
+ * An MLP (in_dim -> `layers` hidden layers of width `hidden`, GELU -> out_dim)
+ * trained and evaluated with the library's BF16 tcgen05 GEMM (FP32
+ * accumulation, FP32 master weights, Adam). All arrays passed as x, y,
+ * target and mask are device memory, row-major, one sample per row. */
+typedef struct dcfr_mlp dcfr_mlp;
+
+int dcfr_mlp_create(int32_t in_dim, int32_t hidden, int32_t layers, int32_t out_dim, int32_t max_batch, uint64_t seed,
+                    dcfr_mlp** out);
+void dcfr_mlp_destroy(dcfr_mlp* n);
+/* Parameter count of the flat layout (per layer W_t[out_pad][in_pad], then
+ * per layer b[out_pad]; every dimension padded to a multiple of 128). */
+int dcfr_mlp_num_params(const dcfr_mlp* n, uint64_t* out);
+int dcfr_mlp_get_params(const dcfr_mlp* n, float* host);
+int dcfr_mlp_set_params(dcfr_mlp* n, const float* host);
+/* y[M][out_dim] = network(x[M][in_dim]). */
+int dcfr_mlp_forward(dcfr_mlp* n, const float* x, int32_t m, float* y);
+/* Loss sum(mask * (y - target)^2) / sum(mask) (mask may be NULL: all ones)
+ * and its gradient in the flat layout (grads_host may be NULL). */
+int dcfr_mlp_gradients(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t m, float* loss,
+                       float* grads_host);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
+int dcfr_mlp_train_step(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t m, float lr,
+                        float* loss);
+/* The tensor-core GEMM itself: c = epi(a[m][k] x b[n][k]^T) with a, b bf16
+ * (k contiguous), m and n multiples of 128, k of 64; epi 0: c f32; 1: c f32
+ * + bias[n]; 2: z bf16 = acc + bias, c bf16 = gelu(z); 3: c bf16 = acc *
+ * gelu'(z). ldc is the row stride of c (and z) in elements. */
+int dcfr_gemm_bf16(const void* a, const void* b, void* c, int32_t m, int32_t n, int32_t k, int32_t epi,
+                   const float* bias, void* z, int32_t ldc, void* stream);
 
 /* Largest hand count per side that dcfr_showdown_values_noalloc accepts. */
 #define DCFR_NOALLOC_MAX_HANDS 1326

@@ -183,6 +183,14 @@ void oracle_nodes(void* h, int32_t* ints, uint64_t* offsets, float* floats, int6
 
 void oracle_iterate(void* h, uint32_t n) { ((Solver*)h)->iterate(n); }
 
+// n iterations of each of count independent solvers, spread over `threads`
+// host threads (one solver per thread at a time, largest first as given):
+// the CPU counterpart of the batched river solve.
+void oracle_batch_iterate(void** hs, int count, uint32_t n, int threads) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1)
+  for (int i = 0; i < count; i++) ((Solver*)hs[i])->iterate(n);
+}
+
 double oracle_exploitability(void* h) { return ((Solver*)h)->exploitability(); }
 
 void oracle_root_values(void* h, double* out) { ((Solver*)h)->root_values(out); }

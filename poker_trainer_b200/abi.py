@@ -129,6 +129,19 @@ class KernelProfile(C.Structure):
     ]
 
 
+class BatchTuning(C.Structure):
+    """dcfr_batch_tuning (include/dcfr.h)."""
+    _fields_ = [
+        ("warps", C.c_int32),
+        ("blocks_per_sm", C.c_int32),
+        ("iterations_per_launch", C.c_uint32),
+        ("longest_first", C.c_int32),
+        ("candidates", C.c_int32),
+        ("_pad", C.c_int32),
+        ("trial_ms", C.c_double),
+    ]
+
+
 class TreeStats(C.Structure):
     _fields_ = [
         ("player_nodes", C.c_uint64),

@@ -16,8 +16,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdcfr.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "engine.cu", "game.cpp", "capi.cpp", "noalloc.cu"]
-HEADERS = ["engine.hpp", "game.hpp", "plan.hpp", os.path.join("..", "..", "include", "dcfr.h")]
+SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "engine.cu", "game.cpp", "capi.cpp", "noalloc.cu", "br64.cu", "batch.cu", "mlp.cu"]
+HEADERS = ["engine.hpp", "game.hpp", "plan.hpp", "warp_terminal.cuh", "row_items.cuh", "batch.hpp", "gemm_tc.cuh", os.path.join("..", "..", "include", "dcfr.h")]
 
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

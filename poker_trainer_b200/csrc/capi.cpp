@@ -7,10 +7,15 @@
 #include <string>
 
 #include "../../include/dcfr.h"
+#include "batch.hpp"
 #include "engine.hpp"
 
 struct dcfr_solver {
   std::unique_ptr<dcfr::Engine> e;
+};
+
+struct dcfr_batch {
+  std::unique_ptr<dcfr::Batch> b;
 };
 
 static thread_local std::string g_error;
@@ -144,6 +149,20 @@ int dcfr_exploitability(dcfr_solver* s, double* out) {
   if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
   GUARD_BEGIN
   return done(s->e->exploitability(*out));
+  GUARD_END
+}
+
+int dcfr_exploitability_fp64(dcfr_solver* s, double* out, double best_response[2]) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  double br[2] = {0.0, 0.0};
+  dcfr::Status st = s->e->exploitability_fp64(*out, br);
+  if (st.ok() && best_response) {
+    best_response[0] = br[0];
+    best_response[1] = br[1];
+  }
+  return done(st);
   GUARD_END
 }
 
@@ -343,6 +362,110 @@ int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profi
   GUARD_BEGIN
   return done(s->e->iterate_profiled(iterations, *out));
   GUARD_END
+}
+
+// ------------------------------------------------------------ batched rivers
+#define NEEDB(h)                                                      \
+  if (!(h) || !(h)->b) return fail(DCFR_ERR_INVALID_ARG, "NULL batch")
+
+int dcfr_batch_create(const dcfr_config* cfgs, int32_t count, dcfr_batch** out) {
+  if (!cfgs || !out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  GUARD_BEGIN
+  std::unique_ptr<dcfr::Batch> b;
+  dcfr::Status st = dcfr::Batch::create(cfgs, count, b);
+  if (!st.ok()) return done(st);
+  *out = new dcfr_batch{std::move(b)};
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+void dcfr_batch_destroy(dcfr_batch* b) { delete b; }
+
+int dcfr_batch_iterate(dcfr_batch* b, uint32_t n) {
+  NEEDB(b);
+  GUARD_BEGIN
+  return done(b->b->iterate(n));
+  GUARD_END
+}
+
+int dcfr_batch_exploitability(dcfr_batch* b, double* out) {
+  NEEDB(b);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");
+  GUARD_BEGIN
+  return done(b->b->exploitability(out));
+  GUARD_END
+}
+
+int dcfr_batch_storage_len(const dcfr_batch* b, int32_t spot, uint64_t* len) {
+  NEEDB(b);
+  if (!len) return fail(DCFR_ERR_INVALID_ARG, "len is NULL");
+  return done(b->b->storage_len(spot, *len));
+}
+
+int dcfr_batch_download_storage(dcfr_batch* b, int32_t spot, float* regrets, float* sums, uint64_t len) {
+  NEEDB(b);
+  uint64_t need = 0;
+  dcfr::Status st = b->b->storage_len(spot, need);
+  if (!st.ok()) return done(st);
+  if (len < need) return fail(DCFR_ERR_INVALID_ARG, "storage buffers are too short");
+  GUARD_BEGIN
+  return done(b->b->download(spot, regrets, sums));
+  GUARD_END
+}
+
+int dcfr_batch_autotune(dcfr_batch* b, uint32_t trial_iterations, dcfr_batch_tuning* out) {
+  NEEDB(b);
+  GUARD_BEGIN
+  dcfr_batch_tuning best{};
+  dcfr::Status st = b->b->autotune(trial_iterations, best);
+  if (st.ok() && out) *out = best;
+  return done(st);
+  GUARD_END
+}
+
+int dcfr_batch_get_tuning(const dcfr_batch* b, dcfr_batch_tuning* out) {
+  NEEDB(b);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");
+  *out = b->b->tuning();
+  return DCFR_OK;
+}
+
+int dcfr_batch_set_tuning(dcfr_batch* b, const dcfr_batch_tuning* t) {
+  NEEDB(b);
+  if (!t) return fail(DCFR_ERR_INVALID_ARG, "tuning is NULL");
+  GUARD_BEGIN
+  return done(b->b->set_tuning(*t));
+  GUARD_END
+}
+
+int dcfr_batch_last_iterate_ms(const dcfr_batch* b, double* ms) {
+  NEEDB(b);
+  if (!ms) return fail(DCFR_ERR_INVALID_ARG, "ms is NULL");
+  *ms = b->b->last_iterate_ms();
+  return DCFR_OK;
+}
+
+int dcfr_batch_iterations(const dcfr_batch* b, uint32_t* out) {
+  NEEDB(b);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");
+  *out = b->b->iterations();
+  return DCFR_OK;
+}
+
+int dcfr_batch_iteration_bytes(const dcfr_batch* b, double* bytes) {
+  NEEDB(b);
+  if (!bytes) return fail(DCFR_ERR_INVALID_ARG, "bytes is NULL");
+  *bytes = b->b->iteration_bytes();
+  return DCFR_OK;
+}
+
+int dcfr_batch_kernel_launches(const dcfr_batch* b, uint64_t* out) {
+  NEEDB(b);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");
+  *out = b->b->kernel_launches();
+  return DCFR_OK;
 }
 
 }  // extern "C"

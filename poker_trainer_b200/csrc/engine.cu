@@ -53,6 +53,7 @@ Plan::~Plan() {
   dfree(d_lanes);
   dfree(d_tasks);
   dfree(d_fast);
+  dfree(d_units);
   dfree(d_trees);
   dfree(d_fdown);
   dfree(d_fup);
@@ -81,6 +82,8 @@ static DiscountD discount_for(uint32_t t, const dcfr_params& prm) {
   d.reach_weighted = prm.unweighted_average ? 0 : 1;
   return d;
 }
+
+DiscountD discount_of(uint32_t t, const dcfr_params& prm) { return discount_for(t, prm); }
 
 // next_check_gap (lib.rs:158-172).
 static uint32_t next_gap(bool has_prev, uint32_t t0, double e0, uint32_t t, double e, double target,
@@ -149,6 +152,9 @@ Engine::~Engine() {
   dfree(fcat_);
   dfree(fseg_);
   dfree(frec_);
+  dfree(reach64_);
+  dfree(vals64_);
+  dfree(root_rows64_);
   dfree(disc_table_);
   dfree(cur_disc_);
   dfree(counter_);
@@ -296,29 +302,7 @@ Status Engine::init() {
       CK(cudaStreamSynchronize(stream_));
       cudaFree(d_boards);
     }
-    if (fast_) {
-      // Scan layouts (terminal_fast.cu): the boards' tables, then the fold layout.
-      fcstride_ = (3 * tstride_ + 7) / 8 * 8;
-      femax_ = fast_emax(tstride_);
-      const size_t nl = (size_t)(nb + 1) * 2;
-      if (!(s = dalloc(fcat_, nl * fcstride_, "scan layouts")).ok()) return s;
-      if (!(s = dalloc(fseg_, nl * FAST_SEGS, "scan layouts")).ok()) return s;
-      if (!(s = dalloc(frec_, nl * tstride_, "scan layouts")).ok()) return s;
-      launch_fast_layouts(tables_, table_count_, tstride_, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1],
-                          fcat_, fseg_, frec_, fcstride_, stream_);
-      CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(stream_));
-      int dev = 0, sms = 0;
-      CK(cudaGetDevice(&dev));
-      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      const int per_sm = fast_blocks_per_sm(stride_, femax_, fcstride_, tstride_);
-      if (per_sm <= 0) {
-        s.code = DCFR_ERR_CUDA;
-        s.msg = "terminal kernel: shared-memory layout does not fit an SM";
-        return s;
-      }
-      fast_blocks_ = sms * per_sm;
-    }
+    if (fast_ && !(s = ensure_fast_layouts()).ok()) return s;
   }
   // Plans for the two traversals of an iteration.
   for (int p = 0; p < 2; p++) {
@@ -362,6 +346,46 @@ Status Engine::init() {
   CK(cudaMemsetAsync(counter_, 0, 4, stream_));
   if (!(s = ensure_discounts(1024)).ok()) return s;
   CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// Scan layouts of the fast terminal kernel (terminal_fast.cu): the boards'
+// strength tables, then the fold layout. Built in init for fast precision,
+// and on first use by the FP64 best-response oracle in exact precision.
+Status Engine::ensure_fast_layouts() {
+  if (fcat_) return Status();
+  Status s;
+  const int nb = (int)g.boards.size();
+  fcstride_ = (3 * tstride_ + 7) / 8 * 8;
+  femax_ = fast_emax(tstride_);
+  const size_t nl = (size_t)(nb + 1) * 2;
+  if (!(s = dalloc(fcat_, nl * fcstride_, "scan layouts")).ok()) return s;
+  if (!(s = dalloc(fseg_, nl * FAST_SEGS, "scan layouts")).ok()) return s;
+  if (!(s = dalloc(frec_, nl * tstride_, "scan layouts")).ok()) return s;
+  launch_fast_layouts(tables_, table_count_, tstride_, nb, hc1_[0], hc2_[0], hc1_[1], hc2_[1], g.n[0], g.n[1], fcat_,
+                      fseg_, frec_, fcstride_, stream_);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(stream_));
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int per_sm = fast_blocks_per_sm(stride_, femax_, fcstride_, tstride_);
+  if (per_sm <= 0) {
+    s.code = DCFR_ERR_CUDA;
+    s.msg = "terminal kernel: shared-memory layout does not fit an SM";
+    return s;
+  }
+  fast_blocks_ = sms * per_sm;
+  for (int k = 0; k < 2; k++) {
+    int bps = 0;
+    term_warps_[k] = warp_terminal_setup(stride_, fcstride_, tstride_, k ? 8 : 4, 16, bps);
+    term_blocks_[k] = sms * bps;
+    if (term_warps_[k] <= 0) {
+      s.code = DCFR_ERR_CUDA;
+      s.msg = "warp terminal kernel: shared-memory layout does not fit an SM";
+      return s;
+    }
+  }
   return Status();
 }
 
@@ -610,6 +634,15 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     for (const TermLane& L : folds[b])
       plan.h_fast.push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, (uint32_t)g.boards.size(),
                                      L.slot, L.row, NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
+  // Units of the warp terminal kernel: runs of at most TERM_UNIT tasks on
+  // one layout (h_fast is ordered by layout within each kind).
+  plan.h_units.clear();
+  for (size_t i = 0; i < plan.h_fast.size();) {
+    size_t j = i;
+    while (j < plan.h_fast.size() && j - i < (size_t)TERM_UNIT && plan.h_fast[j].board == plan.h_fast[i].board) j++;
+    plan.h_units.push_back(TermUnit{plan.h_fast[i].board, (uint32_t)i, (uint32_t)(j - i), 0});
+    i = j;
+  }
   // Terminal tasks: one warp per fold group; per showdown group, the
   // ascending and descending passes and, when a terminal has a paired fold,
   // the paired fold's pass. Launches ("waves") are bounded in tasks and in
@@ -684,6 +717,9 @@ Status Engine::upload_plan(Plan& plan) {
   if (!(s = dalloc(plan.d_lanes, plan.h_lanes.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_tasks, plan.h_tasks.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fast, plan.h_fast.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_units, plan.h_units.size(), "plan")).ok()) return s;
+  if (!plan.h_units.empty())
+    CK(cudaMemcpy(plan.d_units, plan.h_units.data(), plan.h_units.size() * sizeof(TermUnit), cudaMemcpyHostToDevice));
   if (!(s = dalloc(plan.d_trees, plan.h_trees.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fdown, plan.h_fdown.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fup, plan.h_fup.size(), "plan")).ok()) return s;
@@ -799,7 +835,13 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
     if (!plan.h_fast.empty()) {
       FastArgs F;
       fast_args(p, F);
-      launch_fast_terminal(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, stream_);
+      // Warp per terminal for short rows; one block-wide scan per terminal
+      // for long rows, where a warp alone would scan too many elements.
+      if (tstride_ <= WARP_TERMINAL_MAX_HANDS)
+        launch_warp_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), term_warps_[0], term_blocks_[0],
+                             stream_);
+      else
+        launch_fast_terminal(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, stream_);
     }
   } else if (!plan.waves.empty()) {
     TermArgs T;
@@ -998,6 +1040,101 @@ Status Engine::exploitability(double& out) {
 }
 
 Status Engine::root_values(double out[2]) { return mode_root_values(M_AVG, out); }
+
+// Root values of both traversals with double rows (br64.cu): best response
+// (M_BR) or the average strategy (M_AVG); sum over hands of value * weight.
+Status Engine::fp64_root_values(int mode, double out[2]) {
+  Status s;
+  if (!(s = ensure_fast_layouts()).ok()) return s;
+  const size_t N = g.nodes.size();
+  if (!reach64_) {
+    if (!(s = dalloc(reach64_, (size_t)max_slots_ * stride_, "FP64 reach rows")).ok()) return s;
+    if (!(s = dalloc(vals64_, N * (size_t)stride_, "FP64 value rows")).ok()) return s;
+    if (!(s = dalloc(root_rows64_, (size_t)2 * stride_, "FP64 root rows")).ok()) return s;
+    std::vector<double> rr((size_t)2 * stride_, 0.0);
+    for (int p = 0; p < 2; p++)
+      for (int i = 0; i < g.n[p ^ 1]; i++) rr[(size_t)p * stride_ + i] = (double)g.weights[p ^ 1][i];
+    CK(cudaMemcpy(root_rows64_, rr.data(), rr.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemsetAsync(reach64_, 0, (size_t)max_slots_ * stride_ * 8, stream_));
+    CK(cudaMemsetAsync(vals64_, 0, N * (size_t)stride_ * 8, stream_));
+  }
+  std::vector<double> row((size_t)stride_);
+  for (int p = 0; p < 2; p++) {
+    const Plan& plan = *full_[p];
+    const int o = p ^ 1;
+    CK(cudaMemsetAsync(alive_, 0, (size_t)plan.nslots * 4, stream_));
+    CK(cudaMemsetAsync(alive_, 1, 4, stream_));
+    CK(cudaMemcpyAsync(reach64_, root_rows64_ + (size_t)p * stride_, (size_t)stride_ * 8, cudaMemcpyDeviceToDevice,
+                       stream_));
+    Row64Args A;
+    A.sums = sums_;
+    A.reach = reach64_;
+    A.vals = vals64_;
+    A.alive = alive_;
+    for (int q = 0; q < 2; q++) {
+      A.hc1[q] = hc1_[q];
+      A.hc2[q] = hc2_[q];
+      A.n[q] = g.n[q];
+      A.hp[q] = hp_[q];
+    }
+    A.perm = perm_;
+    A.chance_cards = chance_cards_;
+    A.iso = iso_;
+    A.stride = stride_;
+    A.p = p;
+    for (const Plan::Level& l : plan.down)
+      if (l.count) launch_down64(A, plan.d_down + l.first, (int)l.count, hp_[o], stream_);
+    launch_fused_down64(A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fdown, stream_);
+    if (!plan.h_fast.empty()) {
+      FastArgs64 F;
+      F.reach = reach64_;
+      F.vals = vals64_;
+      F.alive = alive_;
+      F.cat = fcat_;
+      F.seg = fseg_;
+      F.rec = frec_;
+      F.same = same_[p];
+      F.cstride = fcstride_;
+      F.tstride = tstride_;
+      F.emax = femax_;
+      for (int q = 0; q < 2; q++) {
+        F.n[q] = g.n[q];
+        F.hp[q] = hp_[q];
+      }
+      F.stride = stride_;
+      F.p = p;
+      launch_warp_terminal64(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), term_warps_[1], term_blocks_[1],
+                             stream_);
+    }
+    launch_fused_up64(mode, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fup, stream_);
+    for (size_t d = plan.up.size(); d-- > 0;) {
+      const Plan::Level& l = plan.up[d];
+      if (l.count) launch_up64(mode, A, plan.d_up + l.first, (int)l.count, hp_[p], stream_);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(row.data(), vals64_ + (size_t)plan.root * stride_, (size_t)stride_ * 8,
+                       cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    double acc = 0.0;
+    for (int h = 0; h < g.n[p]; h++) acc += row[h] * (double)g.weights[p][h];
+    out[p] = acc;
+  }
+  return Status();
+}
+
+// exploitability (cfr.rs:494-502) from the FP64 traversals.
+Status Engine::exploitability_fp64(double& out, double br[2]) {
+  Status s = fp64_root_values(M_BR, br);
+  if (!s.ok()) return s;
+  if (g.cfg.rake_rate > 0.0 && g.cfg.rake_cap > 0.0) {
+    double ev[2];
+    if (!(s = fp64_root_values(M_AVG, ev)).ok()) return s;
+    out = ((br[0] - ev[0]) + (br[1] - ev[1])) / 2.0;
+  } else {
+    out = (br[0] + br[1]) / 2.0;
+  }
+  return Status();
+}
 
 Status Engine::traverse(int p, int mode, uint32_t t, float* out) {
   if (p < 0 || p > 1 || mode < 0 || mode > 2) {

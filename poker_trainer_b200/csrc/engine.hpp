@@ -39,6 +39,18 @@ void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstrid
                          const uint8_t* hc2_0, const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1,
                          uint16_t* cat, uint16_t* seg, uint4* rec, int cstride, cudaStream_t s);
 void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
+void launch_fast_terminal64(const FastArgs64& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
+void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+                          int max_blocks, cudaStream_t s);
+void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+                            int max_blocks, cudaStream_t s);
+int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
+// FP64 best-response oracle kernels (br64.cu).
+void launch_down64(const Row64Args& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s);
+void launch_up64(int mode, const Row64Args& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s);
+void launch_fused_down64(const Row64Args& A, const FusedTree* trees, int ntrees, const DownTask* tasks, cudaStream_t s);
+void launch_fused_up64(int mode, const Row64Args& A, const FusedTree* trees, int ntrees, const UpTask* tasks,
+                       cudaStream_t s);
 int fast_emax(int tstride);
 int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride);
 void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
@@ -70,6 +82,8 @@ struct Plan {
   std::vector<TermLane> h_lanes;
   std::vector<TermTask> h_tasks;
   std::vector<FastTask> h_fast;  // fast precision: one task per terminal
+  std::vector<TermUnit> h_units; // runs of h_fast on one layout (warp terminal kernel)
+  TermUnit* d_units = nullptr;
   // Fused river subtrees (one block each) and their tasks.
   std::vector<FusedTree> h_trees;
   std::vector<DownTask> h_fdown;
@@ -110,6 +124,9 @@ class Engine {
   Status iterate_profiled(uint32_t n, dcfr_kernel_profile& out);
   Status sync();
   Status exploitability(double& out);
+  // The same exploitability with every reach and value row in double
+  // (br64.cu): the FP64 best-response oracle of a solve.
+  Status exploitability_fp64(double& out, double br[2]);
   Status root_values(double out[2]);
   Status traverse(int p, int mode, uint32_t t, float* out);
   Status solve(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb, void* user,
@@ -166,6 +183,14 @@ class Engine {
   uint16_t* fseg_ = nullptr;
   uint4* frec_ = nullptr;
   int fcstride_ = 0, femax_ = 0, fast_blocks_ = 0;
+  // Warp terminal kernel: warps per block and blocks (float rows, double rows).
+  int term_warps_[2] = {0, 0}, term_blocks_[2] = {0, 0};
+  // FP64 best-response rows, allocated on first use.
+  double* reach64_ = nullptr;
+  double* vals64_ = nullptr;
+  double* root_rows64_ = nullptr;
+  Status ensure_fast_layouts();
+  Status fp64_root_values(int mode, double out[2]);
   DiscountD* disc_table_ = nullptr;
   uint32_t disc_len_ = 0;
   DiscountD* cur_disc_ = nullptr;

@@ -125,6 +125,21 @@ struct FastTask {
   double a, b, c, d;  // as TermLane
 };
 
+// A run of fast terminal tasks on one layout, processed by one block of the
+// warp terminal kernel (terminal_fast.cu): the block stages the layout once,
+// then its warps take the run's tasks one per warp.
+constexpr int TERM_UNIT = 16;  // tasks per unit at most
+// Longest opponent hand list evaluated warp per terminal; longer lists use
+// the block-wide scan of fast_terminal_kernel (measured: the block kernel is
+// faster at 1128 hands, the warp kernel at 470).
+constexpr int WARP_TERMINAL_MAX_HANDS = 768;
+struct TermUnit {
+  uint32_t layout;  // FastTask::board of every task in the run
+  uint32_t first;   // first task
+  uint32_t count;   // tasks
+  uint32_t pad;
+};
+
 // Per (layout, traverser) scan layout of the opponent's hands: segment 0
 // lists them in ascending strength, segment 1+c lists those holding card c
 // (ascending strength). seg[j] is the first element of segment j
@@ -135,9 +150,12 @@ struct FastTask {
 constexpr int FAST_SEGS = 54;
 constexpr int FAST_THREADS = 256;
 
-struct FastArgs {
-  const float* reach;
-  float* vals;
+// R is the row type: float for the solve, double for the FP64 best-response
+// oracle (br64.cu).
+template <typename R>
+struct FastArgsT {
+  const R* reach;
+  R* vals;
   const uint32_t* alive;
   const uint16_t* cat;   // [(layout*2+p)][cstride] opponent hand per element
   const uint16_t* seg;   // [(layout*2+p)][FAST_SEGS]
@@ -151,6 +169,8 @@ struct FastArgs {
   int stride;
   int p;
 };
+using FastArgs = FastArgsT<float>;
+using FastArgs64 = FastArgsT<double>;
 
 // Arguments of the row kernels (down/up levels) of one traversal.
 struct RowArgs {
@@ -165,6 +185,24 @@ struct RowArgs {
   const uint8_t* chance_cards;
   const IsoRefD* iso;
   const DiscountD* disc;
+  int n[2];
+  int hp[2];
+  int stride;
+  int p;
+};
+
+// Arguments of the FP64 best-response kernels (br64.cu): double reach and
+// value rows, the f32 strategy sums.
+struct Row64Args {
+  const float* sums;
+  double* reach;
+  double* vals;
+  uint32_t* alive;
+  const uint8_t* hc1[2];
+  const uint8_t* hc2[2];
+  const uint16_t* perm;
+  const uint8_t* chance_cards;
+  const IsoRefD* iso;
   int n[2];
   int hp[2];
   int stride;

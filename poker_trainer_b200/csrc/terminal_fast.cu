@@ -25,18 +25,10 @@
 #include <cstdint>
 
 #include "plan.hpp"
+#include "warp_terminal.cuh"
 
 namespace dcfr {
 
-namespace {
-
-__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
-
-// Fixed-point value of one reach entry: trunc(x * 2^S). Products are exact
-// (power-of-two scale, below 2^52).
-__device__ __forceinline__ long long fixed(float x, double scale) { return __double2ll_rz((double)x * scale); }
-
-}  // namespace
 
 // One thread per (layout, traverser): layouts 0..nboards-1 are the showdown
 // boards' strength tables, layout nboards lists the opponent's hands in hand
@@ -115,19 +107,20 @@ __global__ void fast_layout_kernel(const EntryD* __restrict__ tables, const uint
   }
 }
 
-// Shared-memory layout of a block (all offsets 16-byte aligned).
+// Shared-memory layout of a block (all offsets 16-byte aligned); rsize is
+// the byte size of a row entry (4 for float rows, 8 for double rows).
 struct FastSmem {
   size_t rbuf, r64, g, cs, wsum, fred, cat, rec, same, seg, total;
-  __host__ __device__ FastSmem(int stride, int emax, int cstride, int tstride) {
+  __host__ __device__ FastSmem(int stride, int emax, int cstride, int tstride, int rsize = 4) {
     auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
     const size_t gn = (size_t)FAST_THREADS * emax + 2;
     rbuf = 0;
-    r64 = up16(rbuf + 2 * (size_t)stride * 4);
+    r64 = up16(rbuf + 2 * (size_t)stride * rsize);
     g = up16(r64 + ((size_t)stride + 1) * 8);
     cs = up16(g + gn * 8);
     wsum = up16(cs + 2 * FAST_SEGS * 8);
     fred = up16(wsum + (FAST_THREADS / 32) * 8);
-    cat = up16(fred + 2 * (FAST_THREADS / 32) * 4);
+    cat = up16(fred + 2 * (FAST_THREADS / 32) * rsize);
     rec = up16(cat + (size_t)cstride * 2);
     same = up16(rec + (size_t)tstride * 16);
     seg = up16(same + (size_t)stride * 2);
@@ -147,18 +140,22 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // shared memory when the board changes, and the next task's reach row is
 // copied in (cp.async) while the current one is evaluated. E (elements per
 // thread of the scan, odd) is a compile-time constant so a thread's elements
-// stay in registers between the two passes of the scan.
-template <int E>
-__global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A, const FastTask* __restrict__ tasks,
+// stay in registers between the two passes of the scan. R is the row type:
+// float for the solve, double for the FP64 best-response oracle (br64.cu),
+// whose values are formed in double with no rounding to f32.
+template <int E, typename R>
+__global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
                                                                      int ntasks) {
   extern __shared__ __align__(16) unsigned char smem_fast[];
-  const FastSmem L_(A.stride, E, A.cstride, A.tstride);
-  float* rbuf = reinterpret_cast<float*>(smem_fast + L_.rbuf);
+  constexpr bool F64 = sizeof(R) == 8;
+  constexpr int PER16 = 16 / (int)sizeof(R);  // row entries per 16-byte copy
+  const FastSmem L_(A.stride, E, A.cstride, A.tstride, (int)sizeof(R));
+  R* rbuf = reinterpret_cast<R*>(smem_fast + L_.rbuf);
   long long* R64 = reinterpret_cast<long long*>(smem_fast + L_.r64);
   long long* G = reinterpret_cast<long long*>(smem_fast + L_.g);
   longlong2* Cs = reinterpret_cast<longlong2*>(smem_fast + L_.cs);  // per card: {start prefix, card total}
   long long* wsum = reinterpret_cast<long long*>(smem_fast + L_.wsum);
-  float* fred = reinterpret_cast<float*>(smem_fast + L_.fred);
+  R* fred = reinterpret_cast<R*>(smem_fast + L_.fred);
   uint16_t* scat = reinterpret_cast<uint16_t*>(smem_fast + L_.cat);
   uint4* srec = reinterpret_cast<uint4*>(smem_fast + L_.rec);
   uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_fast + L_.same);
@@ -176,9 +173,9 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
   }
   if (tid == 0) R64[hpo] = 0;
   auto prefetch = [&](int ti, int buf) {
-    const float* src = A.reach + (size_t)tasks[ti].slot * A.stride;
-    float* dst = rbuf + (size_t)buf * A.stride;
-    for (int i = tid; i < hpo / 4; i += FAST_THREADS) cp_async16(dst + 4 * i, src + 4 * i);
+    const R* src = A.reach + (size_t)tasks[ti].slot * A.stride;
+    R* dst = rbuf + (size_t)buf * A.stride;
+    for (int i = tid; i < hpo / PER16; i += FAST_THREADS) cp_async16(dst + PER16 * i, src + PER16 * i);
     cp_async_commit();
   };
   prefetch(t0, 0);
@@ -187,16 +184,23 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
 
   for (int ti = t0; ti < t1; ti++) {
     const int buf = (ti - t0) & 1;
-    const float* r = rbuf + (size_t)buf * A.stride;
+    const R* r = rbuf + (size_t)buf * A.stride;
     // Row ti landed (own copies), partial maxima published.
     cp_async_wait_all();
-    float mx = 0.0f;
-    for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
-      const float4 v = reinterpret_cast<const float4*>(r)[i];
-      mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    R mx = 0;
+    if constexpr (F64) {
+      for (int i = tid; i < hpo / 2; i += FAST_THREADS) {
+        const double2 v = reinterpret_cast<const double2*>(r)[i];
+        mx = row_max(mx, row_max(v.x, v.y));
+      }
+    } else {
+      for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
+        const float4 v = reinterpret_cast<const float4*>(r)[i];
+        mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+      }
     }
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+    for (int d = 16; d > 0; d >>= 1) mx = row_max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
     if (lane == 0) fred[buf * (FAST_THREADS / 32) + warp] = mx;
     __syncthreads();
     if (ti + 1 < t1) prefetch(ti + 1, buf ^ 1);
@@ -216,22 +220,30 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
       const uint4* grec = A.rec + lay * A.tstride;
       for (int h = tid; h < np; h += FAST_THREADS) srec[h] = grec[h];
     }
-    mx = 0.0f;
+    mx = 0;
 #pragma unroll
-    for (int w = 0; w < FAST_THREADS / 32; w++) mx = fmaxf(mx, fred[buf * (FAST_THREADS / 32) + w]);
+    for (int w = 0; w < FAST_THREADS / 32; w++) mx = row_max(mx, fred[buf * (FAST_THREADS / 32) + w]);
     // Row sum < 2048 * 2^(e+1) with 2^e <= max: scale it below 2^62.
-    const int S = 177 - (int)((__float_as_uint(mx) >> 23) & 0xFF);
+    const int S = scale_exponent(mx);
     const double scale = pow2(S), inv = pow2(-S);
     // Payoffs times 2^-S (exact: a power-of-two scaling).
     const double pa = pa0 * inv, pb = pb0 * inv, pc = pc0 * inv, pd = pd0 * inv;
 
     // Reach row as fixed point.
-    for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
-      const float4 v = reinterpret_cast<const float4*>(r)[i];
-      R64[4 * i + 0] = fixed(v.x, scale);
-      R64[4 * i + 1] = fixed(v.y, scale);
-      R64[4 * i + 2] = fixed(v.z, scale);
-      R64[4 * i + 3] = fixed(v.w, scale);
+    if constexpr (F64) {
+      for (int i = tid; i < hpo / 2; i += FAST_THREADS) {
+        const double2 v = reinterpret_cast<const double2*>(r)[i];
+        R64[2 * i + 0] = fixed(v.x, scale);
+        R64[2 * i + 1] = fixed(v.y, scale);
+      }
+    } else {
+      for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
+        const float4 v = reinterpret_cast<const float4*>(r)[i];
+        R64[4 * i + 0] = fixed(v.x, scale);
+        R64[4 * i + 1] = fixed(v.y, scale);
+        R64[4 * i + 2] = fixed(v.z, scale);
+        R64[4 * i + 3] = fixed(v.w, scale);
+      }
     }
     __syncthreads();
 
@@ -280,19 +292,39 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
 
     // Values in hand order. Cs[0] = {0, T0}; Cs[1 + c] = card c.
     const long long T0 = Cs[0].y;
-    float* out = A.vals + (size_t)row * A.stride;
-    float* fout = frow != NONE32 ? A.vals + (size_t)frow * A.stride : nullptr;
+    R* out = A.vals + (size_t)row * A.stride;
+    R* fout = frow != NONE32 ? A.vals + (size_t)frow * A.stride : nullptr;
     const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
     const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
 #pragma unroll 2
     for (int h = tid; h < hpp; h += FAST_THREADS) {
-      float v = 0.0f, fv = 0.0f;
+      R v = 0, fv = 0;
       if (h < np) {
         const uint4 q = srec[h];
         const longlong2 ca = Cs[1 + (q.w & 0xFF)], cb = Cs[1 + ((q.w >> 8) & 0xFF)];
         const long long si = R64[ssame[h]];
         const long long F = T0 - ca.y - cb.y + si;
-        if (fold) {
+        if constexpr (F64) {
+          // Double rows: every value in double, no f32 rounding.
+          if (fold) {
+            v = pa * (double)F;
+          } else {
+            if (q.w >> 16) {
+              const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
+              const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
+              const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
+              const long long W = (Gw + ca.x + cb.x) - Gaw - Gbw;
+              const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+              double res = pa * (double)W + pb * (double)Lx;
+              if (pc0 != 0.0) {
+                const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+                res += pc * (double)eq;
+              }
+              v = res;
+            }
+            if (fout) fv = pd * (double)F;
+          }
+        } else if (fold) {
           // eval_fold (eval.rs:40-64) returns zeros on a zero total.
           v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
         } else {
@@ -328,9 +360,12 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgs A,
 
 template <int E>
 static cudaError_t setup_e(int optin, size_t smem, int& blocks) {
-  cudaError_t e = cudaFuncSetAttribute(fast_terminal_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  cudaError_t e = cudaFuncSetAttribute(fast_terminal_kernel<E, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel<E>, FAST_THREADS, smem);
+  e = cudaFuncSetAttribute(fast_terminal_kernel<E, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel<E, float>, FAST_THREADS, smem);
 }
 
 int fast_emax(int tstride) {
@@ -338,20 +373,20 @@ int fast_emax(int tstride) {
   return e | 1;  // odd: conflict-free strided 8-byte access
 }
 
-size_t fast_smem_bytes(int stride, int emax, int cstride, int tstride) {
-  return FastSmem(stride, emax, cstride, tstride).total;
+size_t fast_smem_bytes(int stride, int emax, int cstride, int tstride, int rsize) {
+  return FastSmem(stride, emax, cstride, tstride, rsize).total;
 }
 
 int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride) {
   int blocks = 0;
-  const size_t smem = fast_smem_bytes(stride, emax, cstride, tstride);
+  const size_t smem = fast_smem_bytes(stride, emax, cstride, tstride, 4);
   // The limit is the device's opt-in maximum (a per-kernel setting shared by
   // every handle), not this handle's size.
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
     return 0;
-  if ((size_t)optin < smem) return 0;
+  if ((size_t)optin < fast_smem_bytes(stride, emax, cstride, tstride, 8)) return 0;
   cudaError_t e = cudaErrorInvalidValue;
   switch (emax) {
 #define FAST_E(e_)                          \
@@ -364,6 +399,131 @@ int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride) {
   return e == cudaSuccess ? blocks : 0;
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-terminal evaluation: the solve's terminal kernel.
+//
+// The same fixed-point prefix sums as fast_terminal_kernel, but every
+// terminal is evaluated by one warp with no block barrier inside a task.
+// A block takes a unit (a run of tasks on one layout), stages that layout in
+// shared memory once, and its warps take the unit's tasks in turn. Per task
+// and warp:
+//   1. the reach row is copied to the warp's shared row (16-byte loads) and
+//      its maximum reduced across the warp, which fixes the scale 2^S;
+//   2. each lane converts E consecutive layout elements to fixed point,
+//      writes them and sums them; a warp shuffle scan turns the lane sums
+//      into exclusive offsets and a second pass rewrites the elements as
+//      exclusive prefixes G;
+//   3. each lane forms the values of hands lane, lane+32, ... from six
+//      prefixes and the four card-segment bounds, exactly as
+//      fast_terminal_kernel does, and stores them coalesced.
+// Shared memory per block: the layout (elements, per-hand records,
+// identical-hand map, segment starts) and, per warp, one row and the
+// prefix array; the warp count W is a launch parameter.
+struct WarpSmem {
+  size_t same, cat, rec, seg, warp0, warp_bytes, row_bytes, total;
+  __host__ __device__ WarpSmem(int stride, int cstride, int tstride, int rsize, int warps) {
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    same = 0;
+    cat = up16(same + (size_t)stride * 2);
+    rec = up16(cat + (size_t)cstride * 2);
+    seg = up16(rec + (size_t)tstride * 16);
+    warp0 = up16(seg + FAST_SEGS * 2);
+    row_bytes = up16((size_t)stride * rsize);
+    warp_bytes = row_bytes + up16(((size_t)cstride + 2) * 8);
+    total = warp0 + (size_t)warps * warp_bytes;
+  }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
+                                                            const TermUnit* __restrict__ units, int nunits) {
+  extern __shared__ __align__(16) unsigned char smem_w[];
+  const int W = (int)blockDim.x >> 5;
+  const WarpSmem L_(A.stride, A.cstride, A.tstride, (int)sizeof(R), W);
+  uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_w + L_.same);
+  uint16_t* scat = reinterpret_cast<uint16_t*>(smem_w + L_.cat);
+  uint4* srec = reinterpret_cast<uint4*>(smem_w + L_.rec);
+  uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_w + L_.seg);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  R* row = reinterpret_cast<R*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes);
+  long long* G = reinterpret_cast<long long*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes + L_.row_bytes);
+
+  const int p = A.p;
+  const int hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
+  for (int h = tid; h < hpp; h += blockDim.x) {
+    const uint32_t sm = h < np ? A.same[h] : NONE32;
+    ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
+  }
+
+  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const TermUnit U = units[u];
+    __syncthreads();  // the previous unit's warps are done with the layout
+    const size_t lay = (size_t)U.layout * 2 + p;
+    const uint16_t* gseg = A.seg + lay * FAST_SEGS;
+    if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
+    const int L = gseg[FAST_SEGS - 1];
+    const uint16_t* gcat = A.cat + lay * A.cstride;
+    for (int k = tid; k < L; k += blockDim.x) scat[k] = gcat[k];
+    const uint4* grec = A.rec + lay * A.tstride;
+    for (int h = tid; h < np; h += blockDim.x) srec[h] = grec[h];
+    __syncthreads();
+    const WarpLayout Y{ssame, scat, srec, sseg, L};
+    for (uint32_t ti = U.first + warp; ti < U.first + U.count; ti += W) {
+      const FastTask T = tasks[ti];
+      if (A.alive[T.slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
+      warp_terminal_task<R>(A, T, Y, row, G, lane);
+    }
+  }
+}
+
+size_t warp_terminal_smem(int stride, int cstride, int tstride, int rsize, int warps) {
+  return WarpSmem(stride, cstride, tstride, rsize, warps).total;
+}
+
+// Warp count (1..max_warps) that maximises resident warps per SM for rows
+// of rsize bytes, and the blocks per SM at that count; 0 if none fits.
+int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm) {
+  int dev = 0, optin = 0;
+  blocks_per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  const void* fn = rsize == 8 ? (const void*)warp_terminal_kernel<double> : (const void*)warp_terminal_kernel<float>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) return 0;
+  int best_w = 0, best_b = 0;
+  for (int w = 1; w <= max_warps; w++) {
+    const size_t smem = warp_terminal_smem(stride, cstride, tstride, rsize, w);
+    if (smem > (size_t)optin) break;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, w * 32, smem) != cudaSuccess) return 0;
+    if (b > 0 && w * b >= best_w * best_b) {
+      best_w = w;
+      best_b = b;
+    }
+  }
+  blocks_per_sm = best_b;
+  return best_w;
+}
+
+template <typename R>
+static void launch_warp_terminal_t(const FastArgsT<R>& A, const FastTask* tasks, const TermUnit* units, int nunits,
+                                   int warps, int max_blocks, cudaStream_t s) {
+  if (nunits <= 0) return;
+  const int blocks = nunits < max_blocks ? nunits : max_blocks;
+  const size_t smem = warp_terminal_smem(A.stride, A.cstride, A.tstride, (int)sizeof(R), warps);
+  warp_terminal_kernel<R><<<blocks, warps * 32, smem, s>>>(A, tasks, units, nunits);
+}
+
+void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+                          int max_blocks, cudaStream_t s) {
+  launch_warp_terminal_t(A, tasks, units, nunits, warps, max_blocks, s);
+}
+
+void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+                            int max_blocks, cudaStream_t s) {
+  launch_warp_terminal_t(A, tasks, units, nunits, warps, max_blocks, s);
+}
+
 void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstride, int nboards, const uint8_t* hc1_0,
                          const uint8_t* hc2_0, const uint8_t* hc1_1, const uint8_t* hc2_1, int n0, int n1,
                          uint16_t* cat, uint16_t* seg, uint4* rec, int cstride, cudaStream_t s) {
@@ -372,18 +532,28 @@ void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstrid
                                                   cat, seg, rec, cstride);
 }
 
-void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s) {
+template <typename R>
+static void launch_fast_terminal_t(const FastArgsT<R>& A, const FastTask* tasks, int ntasks, int max_blocks,
+                                   cudaStream_t s) {
   if (ntasks <= 0) return;
   const int blocks = ntasks < max_blocks ? ntasks : max_blocks;
-  const size_t smem = fast_smem_bytes(A.stride, A.emax, A.cstride, A.tstride);
+  const size_t smem = fast_smem_bytes(A.stride, A.emax, A.cstride, A.tstride, (int)sizeof(R));
   switch (A.emax) {
-#define FAST_E(e_)                                                                  \
-  case e_:                                                                          \
-    fast_terminal_kernel<e_><<<blocks, FAST_THREADS, smem, s>>>(A, tasks, ntasks); \
+#define FAST_E(e_)                                                                     \
+  case e_:                                                                             \
+    fast_terminal_kernel<e_, R><<<blocks, FAST_THREADS, smem, s>>>(A, tasks, ntasks); \
     break;
     FAST_E(1) FAST_E(3) FAST_E(5) FAST_E(7) FAST_E(9) FAST_E(11) FAST_E(13) FAST_E(15) FAST_E(17)
 #undef FAST_E
   }
+}
+
+void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s) {
+  launch_fast_terminal_t(A, tasks, ntasks, max_blocks, s);
+}
+
+void launch_fast_terminal64(const FastArgs64& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s) {
+  launch_fast_terminal_t(A, tasks, ntasks, max_blocks, s);
 }
 
 }  // namespace dcfr

@@ -1,0 +1,183 @@
+// Fixed-point terminal evaluation shared by the terminal kernels
+// (terminal_fast.cu) and the batched river kernel (batch.cu).
+//
+// A terminal's opponent reach row is converted to 64-bit fixed point
+// (scaled by a power of two chosen from the row's maximum so the row sums
+// below 2^62); integer sums are exact and associative, so every sum the
+// reference's evaluators need (crates/solver/src/eval.rs:40-379) is a
+// difference of two prefixes of one scan over the board's layout:
+//   weaker (win)    = G[w] - (card a's weaker part) - (card b's)
+//   stronger (lose) = (T - G[s]) - (card a's stronger part) - (card b's)
+//   equal (tie)     = (G[s] - G[w]) - ... + identical hand (eval.rs:347-379)
+//   fold            = T - (card a total) - (card b total) + identical hand
+// Each integer result is converted to f64 once, scaled back, multiplied by
+// the payoff and, for float rows, rounded to f32 in the evaluator's own
+// combination order (scalar: eval_showdown's two f32 parts; batched:
+// showdown_batch's f64 sum).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.hpp"
+
+namespace dcfr {
+
+__device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// Fixed-point value of one reach entry: trunc(x * 2^S). Products are exact
+// (power-of-two scale, below 2^52).
+__device__ __forceinline__ long long fixed(float x, double scale) { return __double2ll_rz((double)x * scale); }
+__device__ __forceinline__ long long fixed(double x, double scale) { return __double2ll_rz(x * scale); }
+
+// Scale exponent S of a row whose largest entry is mx: mx * 2^S < 2^51, so a
+// row of up to 2048 entries sums below 2^62. For double rows S is capped so
+// 2^S stays finite; entries below 2^-1020 of that cap truncate to zero.
+__device__ __forceinline__ int scale_exponent(float mx) { return 177 - (int)((__float_as_uint(mx) >> 23) & 0xFF); }
+__device__ __forceinline__ int scale_exponent(double mx) {
+  const int e = (int)((__double_as_longlong(mx) >> 52) & 0x7FF);
+  const int S = 1073 - e;
+  return S > 1020 ? 1020 : S;
+}
+__device__ __forceinline__ float row_max(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double row_max(double a, double b) { return fmax(a, b); }
+
+// The staged layout a warp evaluates against: opponent hand per element,
+// per-hand records and segment starts of one (layout, traverser), and the
+// traverser's identical-hand map (0xFFFF: none). L = seg[53] elements.
+struct WarpLayout {
+  const uint16_t* same;
+  const uint16_t* cat;
+  const uint4* rec;
+  const uint16_t* seg;
+  int L;
+};
+
+// One terminal task evaluated by one warp (all 32 lanes call it). row is
+// the warp's shared copy of the reach row (stride entries), G its prefix
+// array (L + 1 entries). The caller has checked the task's slot is live.
+template <typename R>
+__device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const FastTask& T, const WarpLayout& Y, R* row,
+                                                   long long* G, int lane) {
+  constexpr bool F64 = sizeof(R) == 8;
+  constexpr int PER16 = 16 / (int)sizeof(R);
+  const int p = A.p, o = p ^ 1;
+  const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
+  const int L = Y.L;
+  const int E = (((L + 31) >> 5) | 1);  // odd: conflict-free 8-byte strides
+  // 1. Row and its maximum.
+  const R* src = A.reach + (size_t)T.slot * A.stride;
+  R mx = 0;
+  if constexpr (F64) {
+    for (int i = lane; i < hpo / PER16; i += 32) {
+      const double2 v = reinterpret_cast<const double2*>(src)[i];
+      reinterpret_cast<double2*>(row)[i] = v;
+      mx = row_max(mx, row_max(v.x, v.y));
+    }
+  } else {
+    for (int i = lane; i < hpo / PER16; i += 32) {
+      const float4 v = reinterpret_cast<const float4*>(src)[i];
+      reinterpret_cast<float4*>(row)[i] = v;
+      mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) mx = row_max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+  const int S = scale_exponent(mx);
+  const double scale = pow2(S), inv = pow2(-S);
+  const double pa = T.a * inv, pb = T.b * inv, pc = T.c * inv, pd = T.d * inv;
+  __syncwarp();
+  // 2. Elements in layout order, lane sums, exclusive prefixes.
+  const int k0 = lane * E, k1 = min(L, k0 + E);
+  long long local = 0;
+  for (int k = k0; k < k1; k++) {
+    const long long v = fixed(row[Y.cat[k]], scale);
+    G[k] = v;
+    local += v;
+  }
+  long long inc = local;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += y;
+  }
+  long long acc = inc - local;
+  for (int k = k0; k < k1; k++) {
+    const long long v = G[k];
+    G[k] = acc;
+    acc += v;
+  }
+  const long long total = __shfl_sync(0xffffffffu, inc, 31);
+  if (lane == 0) G[L] = total;
+  __syncwarp();
+  // 3. Values in hand order.
+  const long long T0 = G[Y.seg[1]];
+  R* out = A.vals + (size_t)T.row * A.stride;
+  R* fout = T.frow != NONE32 ? A.vals + (size_t)T.frow * A.stride : nullptr;
+  const uint32_t kind = T.kind;
+  const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
+  const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
+  for (int h = lane; h < hpp; h += 32) {
+    R v = 0, fv = 0;
+    if (h < np) {
+      const uint4 q = Y.rec[h];
+      const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
+      const long long a0 = G[Y.seg[1 + a]], b0 = G[Y.seg[1 + b]];
+      const longlong2 ca = make_longlong2(a0, G[Y.seg[2 + a]] - a0);
+      const longlong2 cb = make_longlong2(b0, G[Y.seg[2 + b]] - b0);
+      const uint16_t sm = Y.same[h];
+      const long long si = sm == 0xFFFF ? 0ll : fixed(row[sm], scale);
+      const long long F = T0 - ca.y - cb.y + si;
+      if constexpr (F64) {
+        // Double rows: every value in double, no f32 rounding.
+        if (fold) {
+          v = pa * (double)F;
+        } else {
+          if (q.w >> 16) {
+            const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
+            const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
+            const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
+            const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
+            const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+            double res = pa * (double)Wn + pb * (double)Lx;
+            if (T.c != 0.0) {
+              const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+              res += pc * (double)eq;
+            }
+            v = res;
+          }
+          if (fout) fv = pd * (double)F;
+        }
+      } else if (fold) {
+        // eval_fold (eval.rs:40-64) returns zeros on a zero total.
+        v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
+      } else {
+        if (q.w >> 16) {
+          const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
+          const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
+          const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
+          const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
+          const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+          if (scalar) {
+            v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
+          } else {
+            double res = pa * (double)Wn;
+            res += pb * (double)Lx;
+            v = (float)res;
+          }
+          if (T.c != 0.0) {
+            const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+            v += (float)(pc * (double)eq);
+          }
+        }
+        if (fout) fv = (float)(pd * (double)F);
+      }
+    }
+    out[h] = v;
+    if (fout) fout[h] = fv;
+  }
+  __syncwarp();  // the next task overwrites the row and the prefixes
+}
+
+}  // namespace dcfr

@@ -1,0 +1,133 @@
+"""The leaf-value network over libdcfr's dcfr_mlp_* entry points.
+
+The network is trained and evaluated by the library's own BF16 tcgen05 GEMM
+kernels (FP32 accumulation, FP32 master weights, Adam). torch tensors are
+used here only to hold device memory; every computation runs in libdcfr.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .solver import check, lib
+
+
+def _dev(t):
+    """Device pointer of a contiguous CUDA float32 torch tensor."""
+    import torch
+    assert t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+    return C.c_void_p(t.data_ptr())
+
+
+def _bind():
+    L = lib()
+    if getattr(L, "_mlp_bound", False):
+        return L
+    P = C.c_void_p
+    L.dcfr_mlp_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(P)]
+    L.dcfr_mlp_destroy.argtypes = [P]
+    L.dcfr_mlp_destroy.restype = None
+    L.dcfr_mlp_num_params.argtypes = [P, C.POINTER(C.c_uint64)]
+    L.dcfr_mlp_get_params.argtypes = [P, P]
+    L.dcfr_mlp_set_params.argtypes = [P, P]
+    L.dcfr_mlp_forward.argtypes = [P, P, C.c_int32, P]
+    L.dcfr_mlp_gradients.argtypes = [P, P, P, P, C.c_int32, C.POINTER(C.c_float), P]
+    L.dcfr_mlp_train_step.argtypes = [P, P, P, P, C.c_int32, C.c_float, C.POINTER(C.c_float)]
+    L.dcfr_gemm_bf16.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P]
+    L._mlp_bound = True
+    return L
+
+
+def pad128(x: int) -> int:
+    return (x + 127) // 128 * 128
+
+
+class LeafNet:
+    """MLP in_dim -> layers x hidden (GELU) -> out_dim."""
+
+    def __init__(self, in_dim: int, hidden: int = 1024, layers: int = 4, out_dim: int = 2652, max_batch: int = 1024,
+                 seed: int = 0):
+        L = _bind()
+        h = C.c_void_p()
+        check(L.dcfr_mlp_create(in_dim, hidden, layers, out_dim, max_batch, seed, C.byref(h)))
+        self._h = h
+        self.in_dim, self.hidden, self.layers, self.out_dim, self.max_batch = in_dim, hidden, layers, out_dim, max_batch
+        n = C.c_uint64()
+        check(L.dcfr_mlp_num_params(h, C.byref(n)))
+        self.num_params = n.value
+        self.kin = [pad128(in_dim)] + [hidden] * layers
+        self.nout = [hidden] * layers + [pad128(out_dim)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dcfr_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        check(lib().dcfr_mlp_get_params(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def set_params(self, flat: np.ndarray):
+        flat = np.ascontiguousarray(flat, np.float32)
+        assert flat.size == self.num_params
+        check(lib().dcfr_mlp_set_params(self._h, flat.ctypes.data_as(C.c_void_p)))
+
+    def split(self, flat: np.ndarray):
+        """Views of a flat parameter (or gradient) vector: [(W_t, b)] per layer,
+        W_t padded [nout][kin]."""
+        out, off = [], 0
+        ws = []
+        for k, n in zip(self.kin, self.nout):
+            ws.append(flat[off:off + n * k].reshape(n, k))
+            off += n * k
+        for i, n in enumerate(self.nout):
+            out.append((ws[i], flat[off:off + n]))
+            off += n
+        return out
+
+    def forward(self, x):
+        import torch
+        torch.cuda.synchronize()
+        y = torch.empty((x.shape[0], self.out_dim), dtype=torch.float32, device=x.device)
+        check(lib().dcfr_mlp_forward(self._h, _dev(x), x.shape[0], _dev(y)))
+        return y
+
+    def gradients(self, x, target, mask=None):
+        import torch
+        torch.cuda.synchronize()
+        loss = C.c_float()
+        g = np.zeros(self.num_params, np.float32)
+        check(lib().dcfr_mlp_gradients(self._h, _dev(x), _dev(target), _dev(mask) if mask is not None else None,
+                                       x.shape[0], C.byref(loss), g.ctypes.data_as(C.c_void_p)))
+        return loss.value, g
+
+    def train_step(self, x, target, mask=None, lr: float = 1e-3) -> float:
+        import torch
+        torch.cuda.synchronize()
+        loss = C.c_float()
+        check(lib().dcfr_mlp_train_step(self._h, _dev(x), _dev(target), _dev(mask) if mask is not None else None,
+                                        x.shape[0], lr, C.byref(loss)))
+        return loss.value
+
+
+def gemm_bf16(a, b, epi: int = 0, bias=None, z=None):
+    """c = epi(a @ b^T) with the library's tensor-core kernel; a [m][k] and
+    b [n][k] are CUDA bfloat16 tensors."""
+    import torch
+    L = _bind()
+    m, k = a.shape
+    n = b.shape[0]
+    out_dtype = torch.float32 if epi in (0, 1) else torch.bfloat16
+    c = torch.empty((m, n), dtype=out_dtype, device=a.device)
+    if epi == 2 and z is None:
+        z = torch.empty((m, n), dtype=torch.bfloat16, device=a.device)
+    torch.cuda.synchronize()
+    check(L.dcfr_gemm_bf16(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_void_p(c.data_ptr()), m, n, k, epi,
+                           C.c_void_p(bias.data_ptr()) if bias is not None else None,
+                           C.c_void_p(z.data_ptr()) if z is not None else None, n, None))
+    return c, z

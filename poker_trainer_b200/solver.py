@@ -29,7 +29,13 @@ EXPORTS = [
     "dcfr_actions_at", "dcfr_query_sizes", "dcfr_query", "dcfr_ranges_after", "dcfr_storage_len",
     "dcfr_download_storage", "dcfr_upload_storage", "dcfr_set_iterations", "dcfr_traverse",
     "dcfr_kernel_launches", "dcfr_last_iterate_ms", "dcfr_iteration_bytes", "dcfr_iterate_profiled",
-    "dcfr_showdown_values_noalloc",
+    "dcfr_showdown_values_noalloc", "dcfr_exploitability_fp64",
+    "dcfr_batch_create", "dcfr_batch_destroy", "dcfr_batch_iterate", "dcfr_batch_exploitability",
+    "dcfr_batch_storage_len", "dcfr_batch_download_storage", "dcfr_batch_autotune", "dcfr_batch_get_tuning",
+    "dcfr_batch_set_tuning", "dcfr_batch_last_iterate_ms", "dcfr_batch_iterations", "dcfr_batch_kernel_launches",
+    "dcfr_batch_iteration_bytes",
+    "dcfr_mlp_create", "dcfr_mlp_destroy", "dcfr_mlp_num_params", "dcfr_mlp_get_params", "dcfr_mlp_set_params",
+    "dcfr_mlp_forward", "dcfr_mlp_gradients", "dcfr_mlp_train_step", "dcfr_gemm_bf16",
 ]
 
 
@@ -51,6 +57,21 @@ def lib():
         L.dcfr_iterate.argtypes = [P, C.c_uint32]
         L.dcfr_synchronize.argtypes = [P]
         L.dcfr_exploitability.argtypes = [P, C.POINTER(C.c_double)]
+        L.dcfr_exploitability_fp64.argtypes = [P, C.POINTER(C.c_double), P]
+        L.dcfr_batch_create.argtypes = [P, C.c_int32, C.POINTER(P)]
+        L.dcfr_batch_destroy.argtypes = [P]
+        L.dcfr_batch_destroy.restype = None
+        L.dcfr_batch_iterate.argtypes = [P, C.c_uint32]
+        L.dcfr_batch_exploitability.argtypes = [P, P]
+        L.dcfr_batch_storage_len.argtypes = [P, C.c_int32, C.POINTER(C.c_uint64)]
+        L.dcfr_batch_download_storage.argtypes = [P, C.c_int32, P, P, C.c_uint64]
+        L.dcfr_batch_autotune.argtypes = [P, C.c_uint32, C.POINTER(abi.BatchTuning)]
+        L.dcfr_batch_get_tuning.argtypes = [P, C.POINTER(abi.BatchTuning)]
+        L.dcfr_batch_set_tuning.argtypes = [P, C.POINTER(abi.BatchTuning)]
+        L.dcfr_batch_last_iterate_ms.argtypes = [P, C.POINTER(C.c_double)]
+        L.dcfr_batch_iterations.argtypes = [P, C.POINTER(C.c_uint32)]
+        L.dcfr_batch_kernel_launches.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.dcfr_batch_iteration_bytes.argtypes = [P, C.POINTER(C.c_double)]
         L.dcfr_root_values.argtypes = [P, P]
         L.dcfr_iterations.argtypes = [P, C.POINTER(C.c_uint32)]
         L.dcfr_last_exploitability.argtypes = [P, C.POINTER(C.c_double)]
@@ -261,6 +282,14 @@ class Solver:
         check(lib().dcfr_exploitability(self._h, C.byref(x)))
         return x.value
 
+    def exploitability_fp64(self):
+        """The FP64 best-response oracle: (exploitability, best-response
+        root values of both players), all in chips."""
+        x = C.c_double()
+        br = np.zeros(2, np.float64)
+        check(lib().dcfr_exploitability_fp64(self._h, C.byref(x), _ptr(br)))
+        return x.value, br
+
     def root_values(self) -> np.ndarray:
         out = np.zeros(2, np.float64)
         check(lib().dcfr_root_values(self._h, _ptr(out)))
@@ -396,3 +425,80 @@ class Solver:
         for c, name in enumerate(abi.KERNEL_CLASSES):
             classes[name] = dict(launches=int(prof.launches[c]), ms=float(prof.ms[c]), bytes=float(prof.bytes[c]))
         return dict(iterations=int(prof.iterations), total_ms=float(prof.total_ms), classes=classes)
+
+
+class BatchSolver:
+    """Batched river solves (dcfr_batch_*): many independent river spots
+    solved together by a persistent kernel under a captured CUDA graph."""
+
+    def __init__(self, handle, count):
+        self._h = handle
+        self.count = count
+
+    @staticmethod
+    def new(configs) -> "BatchSolver":
+        arr = (abi.Config * len(configs))(*configs)
+        h = C.c_void_p()
+        check(lib().dcfr_batch_create(arr, len(configs), C.byref(h)))
+        return BatchSolver(h, len(configs))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dcfr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def iterate(self, n: int):
+        check(lib().dcfr_batch_iterate(self._h, n))
+
+    def exploitability(self) -> np.ndarray:
+        out = np.zeros(self.count, np.float64)
+        check(lib().dcfr_batch_exploitability(self._h, _ptr(out)))
+        return out
+
+    def storage_len(self, spot: int) -> int:
+        n = C.c_uint64()
+        check(lib().dcfr_batch_storage_len(self._h, spot, C.byref(n)))
+        return n.value
+
+    def download_storage(self, spot: int):
+        n = self.storage_len(spot)
+        r = np.zeros(n, np.float32)
+        s = np.zeros(n, np.float32)
+        check(lib().dcfr_batch_download_storage(self._h, spot, _ptr(r), _ptr(s), n))
+        return r, s
+
+    def autotune(self, trial_iterations: int = 10) -> abi.BatchTuning:
+        t = abi.BatchTuning()
+        check(lib().dcfr_batch_autotune(self._h, trial_iterations, C.byref(t)))
+        return t
+
+    def tuning(self) -> abi.BatchTuning:
+        t = abi.BatchTuning()
+        check(lib().dcfr_batch_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: abi.BatchTuning):
+        check(lib().dcfr_batch_set_tuning(self._h, C.byref(t)))
+
+    def last_iterate_ms(self) -> float:
+        x = C.c_double()
+        check(lib().dcfr_batch_last_iterate_ms(self._h, C.byref(x)))
+        return x.value
+
+    def iterations(self) -> int:
+        x = C.c_uint32()
+        check(lib().dcfr_batch_iterations(self._h, C.byref(x)))
+        return x.value
+
+    def kernel_launches(self) -> int:
+        x = C.c_uint64()
+        check(lib().dcfr_batch_kernel_launches(self._h, C.byref(x)))
+        return x.value
+
+    def iteration_bytes(self) -> float:
+        x = C.c_double()
+        check(lib().dcfr_batch_iteration_bytes(self._h, C.byref(x)))
+        return x.value

@@ -121,10 +121,12 @@ SIZES = ["33%", "50%", "75%", "100%", "150%"]
 
 def batched_river_spots(count: int = 512, seed: int = 3000, estimate=None, min_nodes=15, max_nodes=400):
     """Independent river spots: 5-card boards from the seed, pot U[400,6000],
-    stack U[2000,15000], 1-3 sizes from {33,50,75,100,150}% plus all-in and a
-    2.5x raise; redrawn until the tree has min_nodes..max_nodes nodes
-    (`estimate(cfg)` gives the node count). Ranges as the river spot with
-    per-spot seeds."""
+    stack U[2000,15000], a menu of 1-3 sizes from {33,50,75,100,150}% plus
+    all-in used for bets and raises alike (max 3 bets); redrawn until the
+    tree has min_nodes..max_nodes nodes (`estimate(cfg)` gives the node
+    count). The sizes serve raises too because a single 2.5x raise caps
+    these trees at 63 nodes, short of the 15-400 spread the workload asks
+    for. Ranges as the river spot with per-spot seeds."""
     rng = np.random.default_rng(seed)
     out = []
     while len(out) < count:
@@ -136,7 +138,7 @@ def batched_river_spots(count: int = 512, seed: int = 3000, estimate=None, min_n
         bet = [SIZES[i] for i in sizes] + ["allin"]
         i = len(out)
         cfg = abi.make_config(board, [uniform_range(seed + 2 * i + 1), uniform_range(seed + 2 * i + 2)], pot=pot,
-                              stack=stack, menu_=abi.menu(bet, ["2.5x"], max_raises=3),
+                              stack=stack, menu_=abi.menu(bet, bet, max_raises=3),
                               storage=abi.STORAGE_F32, **DCFR)
         if estimate is not None:
             n = estimate(cfg)
