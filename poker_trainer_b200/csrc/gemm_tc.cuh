@@ -29,7 +29,7 @@ namespace dcfr {
 constexpr int GEMM_BM = 128, GEMM_BN = 128, GEMM_BK = 64, GEMM_STAGES = 4, GEMM_THREADS = 128;
 constexpr uint32_t GEMM_TILE_BYTES = GEMM_BM * GEMM_BK * 2;  // one 128 x 64 bf16 tile
 constexpr size_t GEMM_SMEM = 1024 + 2 * GEMM_STAGES * (size_t)GEMM_TILE_BYTES + 256;
-constexpr long long GEMM_WAIT_LIMIT = 1ll << 26;  // polls before a wait gives up
+constexpr long long GEMM_WAIT_LIMIT = 1ll << 22;  // polls before a wait gives up (well over a second)
 
 // Epilogues.
 enum GemmEpi : int {
