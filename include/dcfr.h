@@ -254,6 +254,27 @@ int dcfr_exploitability(dcfr_solver* s, double* out);
  * NULL) receives each player's best-response root value in chips. The first
  * call allocates the double rows on the device. */
 int dcfr_exploitability_fp64(dcfr_solver* s, double* out, double best_response[2]);
+/* No counterpart in the reference: a depth-limited flop solve. The tree of a
+ * flop-root config ends at the turn deal, and every traversal values those
+ * leaves with the leaf-value network `net` (dcfr_mlp_*, 2706 inputs, 2652
+ * outputs, max batch at least leaves x 49): for each dealt card the network
+ * gives every combo's EV in pots from both players' ranges, the board, pot
+ * and stack, and the leaf sums them as a chance node sums its children.
+ * Fast precision, no rake. net must outlive the solver; everything else
+ * (dcfr_iterate, dcfr_solve, queries, exploitability of the depth-limited
+ * game) works as for dcfr_create. */
+typedef struct dcfr_mlp dcfr_mlp;
+int dcfr_create_depth_limited(const dcfr_config* cfg, dcfr_mlp* net, dcfr_solver** out);
+/* Offset, action count and hand count of the decision node at `path` in the
+ * reference storage layout (Node::offset, tree.rs:200-204): its block in
+ * dcfr_download_storage / dcfr_upload_storage arrays. */
+int dcfr_node_storage(dcfr_solver* s, const dcfr_step* path, size_t n, uint64_t* offset, int32_t* num_actions,
+                      int32_t* num_hands);
+/* Overwrites the regrets and/or strategy sums (either may be NULL) of the
+ * decision node at `path` from [num_actions][num_hands] blocks in the
+ * reference layout; e.g. to judge a depth-limited solve's flop strategy
+ * inside a full tree. */
+int dcfr_write_node(dcfr_solver* s, const dcfr_step* path, size_t n, const float* regrets, const float* sums);
 /* Solver::root_values (lib.rs:468-470): average-strategy EV of each player. */
 int dcfr_root_values(dcfr_solver* s, double out[2]);
 /* Solver::iterations, last_exploitability, stats, root_pot. */
@@ -377,8 +398,6 @@ int dcfr_batch_iteration_bytes(const dcfr_batch* b, double* bytes);
  * trained and evaluated with the library's BF16 tcgen05 GEMM (FP32
  * accumulation, FP32 master weights, Adam). All arrays passed as x, y,
  * target and mask are device memory, row-major, one sample per row. */
-typedef struct dcfr_mlp dcfr_mlp;
-
 int dcfr_mlp_create(int32_t in_dim, int32_t hidden, int32_t layers, int32_t out_dim, int32_t max_batch, uint64_t seed,
                     dcfr_mlp** out);
 void dcfr_mlp_destroy(dcfr_mlp* n);

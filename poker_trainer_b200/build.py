@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdcfr.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "engine.cu", "game.cpp", "capi.cpp", "noalloc.cu", "br64.cu", "batch.cu", "mlp.cu"]
+SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "engine.cu", "game.cpp", "capi.cpp", "noalloc.cu", "br64.cu", "batch.cu", "mlp.cu", "leaf.cu"]
 HEADERS = ["engine.hpp", "game.hpp", "plan.hpp", "warp_terminal.cuh", "row_items.cuh", "batch.hpp", "gemm_tc.cuh", os.path.join("..", "..", "include", "dcfr.h")]
 
 FLAGS = [

@@ -88,7 +88,7 @@ struct BatchSmem {
     seg = up16(rec + (size_t)tstride * 16);
     warp0 = up16(seg + FAST_SEGS * 2);
     row_bytes = up16((size_t)max_stride * 4);
-    warp_bytes = row_bytes + up16(((size_t)cstride + 2) * 8);
+    warp_bytes = row_bytes + up16(warp_prefix_entries(cstride) * 8);
     total = warp0 + (size_t)warps * warp_bytes;
   }
 };

@@ -166,6 +166,40 @@ int dcfr_exploitability_fp64(dcfr_solver* s, double* out, double best_response[2
   GUARD_END
 }
 
+int dcfr_create_depth_limited(const dcfr_config* cfg, dcfr_mlp* net, dcfr_solver** out) {
+  if (!cfg || !out || !net) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  GUARD_BEGIN
+  std::unique_ptr<dcfr::Engine> e;
+  dcfr::Status st = dcfr::Engine::create_depth_limited(*cfg, net, DCFR_TURN, e);
+  if (!st.ok()) return done(st);
+  *out = new dcfr_solver{std::move(e)};
+  g_error.clear();
+  return DCFR_OK;
+  GUARD_END
+}
+
+int dcfr_node_storage(dcfr_solver* s, const dcfr_step* path, size_t n, uint64_t* offset, int32_t* num_actions,
+                      int32_t* num_hands) {
+  NEED(s);
+  if (!offset || !num_actions || !num_hands) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  GUARD_BEGIN
+  int na = 0, nh = 0;
+  dcfr::Status st = s->e->node_storage(steps(path, n), *offset, na, nh);
+  *num_actions = na;
+  *num_hands = nh;
+  return done(st);
+  GUARD_END
+}
+
+int dcfr_write_node(dcfr_solver* s, const dcfr_step* path, size_t n, const float* regrets, const float* sums) {
+  NEED(s);
+  if (!regrets && !sums) return fail(DCFR_ERR_INVALID_ARG, "nothing to write");
+  GUARD_BEGIN
+  return done(s->e->write_node(steps(path, n), regrets, sums));
+  GUARD_END
+}
+
 int dcfr_root_values(dcfr_solver* s, double out[2]) {
   NEED(s);
   if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");

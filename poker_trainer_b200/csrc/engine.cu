@@ -54,6 +54,7 @@ Plan::~Plan() {
   dfree(d_tasks);
   dfree(d_fast);
   dfree(d_units);
+  dfree(d_leaves);
   dfree(d_trees);
   dfree(d_fdown);
   dfree(d_fup);
@@ -117,6 +118,27 @@ Status Engine::create(const dcfr_config& cfg, std::unique_ptr<Engine>& out) {
   return Status();
 }
 
+Status Engine::create_depth_limited(const dcfr_config& cfg, dcfr_mlp* net, int leaf_street,
+                                    std::unique_ptr<Engine>& out) {
+  std::unique_ptr<Engine> e(new Engine());
+  Status s;
+  if (!net) return Status{DCFR_ERR_INVALID_ARG, "depth-limited solve: NULL network"};
+  if (cfg.board_len != 3 || cfg.root.street != DCFR_FLOP || leaf_street != DCFR_TURN)
+    return Status{DCFR_ERR_UNSUPPORTED, "depth-limited solves take a flop root cut at the turn deal"};
+  if (cfg.precision != DCFR_PRECISION_FAST)
+    return Status{DCFR_ERR_UNSUPPORTED, "depth-limited solves run in fast precision"};
+  if (cfg.rake_rate > 0.0 && cfg.rake_cap > 0.0)
+    return Status{DCFR_ERR_UNSUPPORTED, "depth-limited solves take unraked games"};
+  e->fast_ = true;
+  s.code = build_game(cfg, e->g, s.msg, true, leaf_street);
+  if (!s.ok()) return s;
+  e->net_ = net;
+  if (!(s = e->init()).ok()) return s;
+  if (!(s = e->init_leaves()).ok()) return s;
+  out = std::move(e);
+  return Status();
+}
+
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   free_graphs();
@@ -152,6 +174,12 @@ Engine::~Engine() {
   dfree(fcat_);
   dfree(fseg_);
   dfree(frec_);
+  for (int q = 0; q < 2; q++) {
+    dfree(leaf_reach_[q]);
+    dfree(combos_[q]);
+  }
+  dfree(leaf_x_);
+  dfree(leaf_cards_);
   dfree(reach64_);
   dfree(vals64_);
   dfree(root_rows64_);
@@ -514,6 +542,10 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
                  (uint32_t)g.chance[nd.index].ci.size(), 0};
         up[depth].push_back(u);
       }
+    } else if (nd.kind == N_LEAF) {
+      // Depth-limited cut: valued by the leaf-value network (leaf.cu).
+      const Game::Leaf& lf = g.leaves[nd.index];
+      plan.h_leaves.push_back(LeafTask{nd.index, sv, v, 0, (float)lf.pot, (float)lf.stack});
     } else {
       // Terminal. Batched evaluation (river.rs) iff the terminal sits below a
       // river decision node inside this traversal (cfr.rs:282-284).
@@ -718,6 +750,10 @@ Status Engine::upload_plan(Plan& plan) {
   if (!(s = dalloc(plan.d_tasks, plan.h_tasks.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fast, plan.h_fast.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_units, plan.h_units.size(), "plan")).ok()) return s;
+  if (!(s = dalloc(plan.d_leaves, plan.h_leaves.size(), "plan")).ok()) return s;
+  if (!plan.h_leaves.empty())
+    CK(cudaMemcpy(plan.d_leaves, plan.h_leaves.data(), plan.h_leaves.size() * sizeof(LeafTask),
+                  cudaMemcpyHostToDevice));
   if (!plan.h_units.empty())
     CK(cudaMemcpy(plan.d_units, plan.h_units.data(), plan.h_units.size() * sizeof(TermUnit), cudaMemcpyHostToDevice));
   if (!(s = dalloc(plan.d_trees, plan.h_trees.size(), "plan")).ok()) return s;
@@ -849,6 +885,7 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
     for (const Plan::Wave& w : plan.waves)
       launch_terminal(T, plan.d_groups, plan.d_lanes, plan.d_tasks + w.first, (int)w.count, stream_);
   }
+  enqueue_leaves(plan);
   mark(DCFR_KERNEL_TERMINAL);
   launch_fused_up(mode, plan.fused_maxa, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fup, hp_[p], stream_);
   for (size_t d = plan.up.size(); d-- > 0;) {
@@ -859,6 +896,124 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   if (root_out)
     cudaMemcpyAsync(root_out, vals_ + (size_t)plan.root * stride_, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice,
                     stream_);
+}
+
+// Depth-limited solves: buffers of the leaf evaluation, and both players'
+// ranges at the leaves from one pass of average-strategy traversals (the
+// strategy sums are zero at creation: uniform strategies).
+Status Engine::init_leaves() {
+  Status s;
+  const int L = (int)g.leaves.size();
+  std::vector<uint8_t> cards;
+  uint64_t used = 0;
+  for (int c : g.board) used |= 1ull << c;
+  for (int c = 0; c < 52; c++)
+    if (!(used >> c & 1)) cards.push_back((uint8_t)c);
+  leaf_nc_ = (int)cards.size();
+  // Chance factor of the deal at the leaves, as a chance node's (tree.rs:520-542):
+  // 1 / (cards * compatible / available) in f32.
+  const float compatible = (float)(52 - (int)g.board.size() - 4);
+  leaf_factor_ = 1.0f / ((float)leaf_nc_ * compatible / (float)leaf_nc_);
+  int in_dim = 0, out_dim = 0, max_batch = 0;
+  if (mlp_shape(net_, &in_dim, &out_dim, &max_batch))
+    return Status{DCFR_ERR_INVALID_ARG, "depth-limited solve: invalid network"};
+  if (in_dim != 2 * DCFR_NUM_COMBOS + 54 || out_dim != 2 * DCFR_NUM_COMBOS)
+    return Status{DCFR_ERR_INVALID_ARG, "leaf network must map 2706 inputs to 2652 outputs"};
+  if (max_batch < std::max(L, 1) * leaf_nc_)
+    return Status{DCFR_ERR_INVALID_ARG, "leaf network batch is smaller than leaves x dealt cards (" +
+                                            std::to_string(L * leaf_nc_) + ")"};
+  for (int q = 0; q < 2; q++) {
+    if (!(s = dalloc(leaf_reach_[q], (size_t)std::max(L, 1) * stride_, "leaf ranges")).ok()) return s;
+    CK(cudaMemsetAsync(leaf_reach_[q], 0, (size_t)std::max(L, 1) * stride_ * 4, stream_));
+    std::vector<uint16_t> cb(hp_[q], 0);
+    for (int i = 0; i < g.n[q]; i++) cb[i] = g.combos[q][i];
+    if (!(s = dalloc(combos_[q], cb.size(), "leaf combos")).ok()) return s;
+    CK(cudaMemcpy(combos_[q], cb.data(), cb.size() * 2, cudaMemcpyHostToDevice));
+  }
+  if (!(s = dalloc(leaf_x_, (size_t)std::max(L, 1) * leaf_nc_ * (2 * DCFR_NUM_COMBOS + 54), "leaf inputs")).ok())
+    return s;
+  if (!(s = dalloc(leaf_cards_, cards.size(), "leaf cards")).ok()) return s;
+  CK(cudaMemcpy(leaf_cards_, cards.data(), cards.size(), cudaMemcpyHostToDevice));
+  for (int p = 0; p < 2; p++)
+    enqueue_traversal(*full_[p], M_AVG, root_rows_ + (size_t)p * stride_, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(stream_));
+  return leaf_status_;
+}
+
+void Engine::enqueue_leaves(const Plan& plan) {
+  if (!net_ || plan.h_leaves.empty()) return;
+  const int p = plan.p, o = p ^ 1;
+  LeafArgs A;
+  A.reach = reach_;
+  A.vals = vals_;
+  A.alive = alive_;
+  for (int q = 0; q < 2; q++) {
+    A.leaf_reach[q] = leaf_reach_[q];
+    A.combos[q] = combos_[q];
+    A.n[q] = g.n[q];
+  }
+  A.x = leaf_x_;
+  A.y = nullptr;
+  A.ldy = 0;
+  A.cards = leaf_cards_;
+  A.nc = leaf_nc_;
+  for (int k = 0; k < 3; k++) A.board[k] = g.board[k];
+  A.stride = stride_;
+  A.p = p;
+  A.factor = leaf_factor_;
+  A.norm = g.norm;
+  const int nl = (int)plan.h_leaves.size();
+  launch_leaf_capture(A, plan.d_leaves, nl, stream_);
+  launch_leaf_inputs(A, plan.d_leaves, nl, hc1_[0], hc2_[0], hc1_[1], hc2_[1], stream_);
+  const float* y = nullptr;
+  int ldy = 0;
+  if (mlp_enqueue_forward(net_, leaf_x_, (int)g.leaves.size() * leaf_nc_, stream_, &y, &ldy) != DCFR_OK) {
+    leaf_status_ = Status{DCFR_ERR_CUDA, "leaf network forward pass failed"};
+    return;
+  }
+  A.y = y;
+  A.ldy = ldy;
+  launch_leaf_values(A, plan.d_leaves, nl, hc1_[p], hc2_[p], hc1_[o], hc2_[o], hp_[p], stream_);
+}
+
+static Status bad_path(const std::string& m);
+
+Status Engine::node_storage(const std::vector<dcfr_step>& path, uint64_t& offset, int& num_actions, int& num_hands) {
+  std::vector<float> reach[2];
+  std::vector<uint32_t> to_canon[2];
+  uint32_t node = 0;
+  Status s = walk(path, node, reach, to_canon);
+  if (!s.ok()) return s;
+  const GNode& nd = g.nodes[node];
+  if (nd.kind != N_PLAYER) return bad_path("not a decision node");
+  offset = nd.ref_offset;
+  num_actions = nd.nchild;
+  num_hands = g.n[nd.player];
+  return Status();
+}
+
+// Overwrites one decision node's strategy sums (and regrets, if given) from
+// blocks in the reference layout ([actions][hands]).
+Status Engine::write_node(const std::vector<dcfr_step>& path, const float* regrets, const float* sums) {
+  std::vector<float> reach[2];
+  std::vector<uint32_t> to_canon[2];
+  uint32_t node = 0;
+  Status s = walk(path, node, reach, to_canon);
+  if (!s.ok()) return s;
+  const GNode& nd = g.nodes[node];
+  if (nd.kind != N_PLAYER) return bad_path("not a decision node");
+  const int q = nd.player, n = g.n[q];
+  for (int a = 0; a < nd.nchild; a++) {
+    if (sums)
+      CK(cudaMemcpyAsync(sums_ + gpu_off_[node] + (size_t)a * hp_[q], sums + (size_t)a * n, (size_t)n * 4,
+                         cudaMemcpyHostToDevice, stream_));
+    if (regrets)
+      CK(cudaMemcpyAsync(regrets_ + gpu_off_[node] + (size_t)a * hp_[q], regrets + (size_t)a * n, (size_t)n * 4,
+                         cudaMemcpyHostToDevice, stream_));
+  }
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
 }
 
 Status Engine::ensure_discounts(uint32_t max_t) {
@@ -996,6 +1151,7 @@ Status Engine::iterate(uint32_t n) {
   CK(cudaEventRecord(ev1_, stream_));
   iterations += n;
   CK(cudaEventSynchronize(ev1_));
+  if (!leaf_status_.ok()) return leaf_status_;
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
   last_iterate_ms = ms;

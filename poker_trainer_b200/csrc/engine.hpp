@@ -12,6 +12,8 @@
 #include "game.hpp"
 #include "plan.hpp"
 
+struct dcfr_mlp;
+
 namespace dcfr {
 
 struct RowArgs;
@@ -84,6 +86,8 @@ struct Plan {
   std::vector<FastTask> h_fast;  // fast precision: one task per terminal
   std::vector<TermUnit> h_units; // runs of h_fast on one layout (warp terminal kernel)
   TermUnit* d_units = nullptr;
+  std::vector<LeafTask> h_leaves; // depth-limited solves: the leaves of this traversal
+  LeafTask* d_leaves = nullptr;
   // Fused river subtrees (one block each) and their tasks.
   std::vector<FusedTree> h_trees;
   std::vector<DownTask> h_fdown;
@@ -109,9 +113,42 @@ struct Plan {
   ~Plan();
 };
 
+// Leaf evaluation of depth-limited solves (leaf.cu).
+struct LeafArgs {
+  const float* reach;       // reach rows (slots x stride)
+  float* vals;              // value rows (nodes x stride)
+  const uint32_t* alive;
+  float* leaf_reach[2];     // per player: its reach at each leaf [leaves][stride], hand order
+  const uint16_t* combos[2];// per player: combo id of each hand
+  float* x;                 // network input [leaves * nc][in_dim]
+  const float* y;           // network output, row stride ldy: EV / pot per combo, player 0 then 1
+  int ldy;
+  const uint8_t* cards;     // the nc cards dealt at the leaves (ascending)
+  int nc;
+  int board[3];
+  int n[2];
+  int stride;
+  int p;
+  float factor;             // chance factor of the leaf's deal (tree.rs:520-542)
+  double norm;              // 1 / num_combinations
+};
+void launch_leaf_capture(const LeafArgs& A, const LeafTask* tasks, int ntasks, cudaStream_t s);
+void launch_leaf_inputs(const LeafArgs& A, const LeafTask* tasks, int ntasks, const uint8_t* hc1_0,
+                        const uint8_t* hc2_0, const uint8_t* hc1_1, const uint8_t* hc2_1, cudaStream_t s);
+void launch_leaf_values(const LeafArgs& A, const LeafTask* tasks, int ntasks, const uint8_t* hc1_p,
+                        const uint8_t* hc2_p, const uint8_t* hc1_o, const uint8_t* hc2_o, int hp, cudaStream_t s);
+// The leaf-value network (mlp.cu): shape check, and a forward pass enqueued on
+// stream s (no synchronisation) whose padded output y has row stride ldy.
+int mlp_shape(const dcfr_mlp* n, int* in_dim, int* out_dim, int* max_batch);
+int mlp_enqueue_forward(dcfr_mlp* n, const float* x, int m, cudaStream_t s, const float** y, int* ldy);
+
 class Engine {
  public:
   static Status create(const dcfr_config& cfg, std::unique_ptr<Engine>& out);
+  // A depth-limited solve: the tree ends at the deal of leaf_street, whose
+  // nodes are valued by `net` (not owned; must outlive the solver).
+  static Status create_depth_limited(const dcfr_config& cfg, dcfr_mlp* net, int leaf_street,
+                                     std::unique_ptr<Engine>& out);
   ~Engine();
 
   Game g;
@@ -141,6 +178,11 @@ class Engine {
   Status actions_at(const std::vector<dcfr_step>& path, std::vector<Act>& out, bool& decision);
   double iteration_bytes() const;
   int isomorphic_pairs() const;
+  // Offset of a decision node's block in the reference storage layout.
+  Status node_storage(const std::vector<dcfr_step>& path, uint64_t& offset, int& num_actions, int& num_hands);
+  bool depth_limited() const { return net_ != nullptr; }
+  // Overwrites a decision node's blocks (reference layout [actions][hands]).
+  Status write_node(const std::vector<dcfr_step>& path, const float* regrets, const float* sums);
 
  private:
   cudaStream_t stream_ = nullptr;
@@ -185,6 +227,17 @@ class Engine {
   int fcstride_ = 0, femax_ = 0, fast_blocks_ = 0;
   // Warp terminal kernel: warps per block and blocks (float rows, double rows).
   int term_warps_[2] = {0, 0}, term_blocks_[2] = {0, 0};
+  // Depth-limited solves: the leaf-value network and its buffers.
+  dcfr_mlp* net_ = nullptr;
+  float* leaf_reach_[2] = {nullptr, nullptr};
+  float* leaf_x_ = nullptr;
+  uint8_t* leaf_cards_ = nullptr;
+  uint16_t* combos_[2] = {nullptr, nullptr};
+  int leaf_nc_ = 0;
+  float leaf_factor_ = 0.0f;
+  Status init_leaves();
+  void enqueue_leaves(const Plan& plan);
+  Status leaf_status_;
   // FP64 best-response rows, allocated on first use.
   double* reach64_ = nullptr;
   double* vals64_ = nullptr;

@@ -244,7 +244,7 @@ static void count_player(Ctx& cx, const Betting& st, std::vector<int>& dealt, St
 // count_after_street (tree.rs:364-401): without isomorphism every runout's
 // subtree has the same size, so one stands for all.
 static void count_street_over(Ctx& cx, const Betting& st, std::vector<int>& dealt, Stats& s) {
-  if (st.street == DCFR_RIVER) {
+  if (st.street == DCFR_RIVER || (cx.g->leaf_street >= 0 && st.street + 1 >= cx.g->leaf_street)) {
     s.terminal++;
     return;
   }
@@ -324,6 +324,16 @@ static void fill_player(Ctx& cx, uint32_t id, const Betting& st, int32_t i0, int
 // Builder::fill_after_street (tree.rs:501-560) and table_for (562-573).
 static void fill_street_over(Ctx& cx, uint32_t id, const Betting& st, int32_t i0, int32_t i1, std::vector<int>& dealt) {
   Game& g = *cx.g;
+  if (g.leaf_street >= 0 && st.street + 1 >= g.leaf_street && st.street != DCFR_RIVER) {
+    GNode& nd = g.nodes[id];
+    nd.kind = N_LEAF;
+    nd.street = (uint8_t)st.street;
+    nd.invest[0] = i0;
+    nd.invest[1] = i1;
+    nd.index = (uint32_t)g.leaves.size();
+    g.leaves.push_back(Game::Leaf{id, st.pot, std::min(st.stack[0], st.stack[1])});
+    return;
+  }
   if (st.street == DCFR_RIVER) {
     uint64_t key = 0;
     for (int c : dealt) key |= 1ull << c;
@@ -505,8 +515,10 @@ void normalize_rows(float* s, int na, int n) {
   }
 }
 
-int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tree) {
+int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tree, int leaf_street) {
   g.cfg = cfg;
+  g.leaf_street = leaf_street;
+  g.leaves.clear();
   int nb = cfg.board_len;
   if (nb < 3 || nb > 5) {
     msg = "invalid board: " + std::to_string(nb) + " cards";

@@ -17,7 +17,9 @@
 
 namespace dcfr {
 
-enum : uint8_t { N_PLAYER = 0, N_CHANCE = 1, N_FOLD = 2, N_SHOWDOWN = 3 };
+// N_LEAF: a depth-limited solve's cut (the deal of leaf_street), valued by
+// the leaf-value network instead of a subtree.
+enum : uint8_t { N_PLAYER = 0, N_CHANCE = 1, N_FOLD = 2, N_SHOWDOWN = 3, N_LEAF = 4 };
 constexpr uint32_t NO = 0xFFFFFFFFu;
 
 struct Act {
@@ -85,12 +87,20 @@ struct Game {
   uint32_t player_nodes = 0;
   Stats stats;
   bool compressed = false;
+  // Depth limit: the deal of this street ends the tree in N_LEAF nodes
+  // (-1: no limit). Leaves in creation order: node id, pot, effective stack.
+  int leaf_street = -1;
+  struct Leaf {
+    uint32_t node;
+    int64_t pot, stack;
+  };
+  std::vector<Leaf> leaves;
 
   std::vector<Act> actions(uint32_t id) const;
 };
 
 // Builds everything; on failure returns a DCFR_ERR_* code and a message.
-int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tree);
+int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tree, int leaf_street = -1);
 
 // Memory estimate of the reference (TreeStats::memory_bytes, tree.rs:264-268).
 uint64_t reference_memory_bytes(const Stats& s, bool compressed);

@@ -258,17 +258,19 @@ int refresh_bf16(dcfr_mlp* n) {
   return DCFR_OK;
 }
 
-int forward(dcfr_mlp* n, const float* x, int M, int Mp) {
+int forward(dcfr_mlp* n, const float* x, int M, int Mp, cudaStream_t s) {
   int rc;
-  pack_bf16<<<blocks_for((size_t)Mp * n->kin[0], 256), 256, 0, n->stream>>>(x, M, n->in_dim, n->X[0], Mp, n->kin[0]);
+  pack_bf16<<<blocks_for((size_t)Mp * n->kin[0], 256), 256, 0, s>>>(x, M, n->in_dim, n->X[0], Mp, n->kin[0]);
   for (int l = 0; l < n->layers; l++)
     if ((rc = gemm(n->X[l], n->wt_bf[l], Mp, n->nout[l], n->kin[l], EPI_BIAS_GELU, n->X[l + 1], n->nout[l], n->Z[l],
-                   n->w + n->boff[l], n->err, n->stream)))
+                   n->w + n->boff[l], n->err, s)))
       return rc;
   const int L = n->layers;
   return gemm(n->X[L], n->wt_bf[L], Mp, n->nout[L], n->kin[L], EPI_BIAS_F32, n->Y, n->nout[L], nullptr,
-              n->w + n->boff[L], n->err, n->stream);
+              n->w + n->boff[L], n->err, s);
 }
+
+int forward(dcfr_mlp* n, const float* x, int M, int Mp) { return forward(n, x, M, Mp, n->stream); }
 
 // Gradients of the loss into n->g (and the loss into n->loss).
 int backward(dcfr_mlp* n, const float* target, const float* mask, int M, int Mp) {
@@ -314,6 +316,30 @@ int batch_ok(dcfr_mlp* n, int M) {
 }
 
 }  // namespace
+
+namespace dcfr {
+
+int mlp_shape(const dcfr_mlp* n, int* in_dim, int* out_dim, int* max_batch) {
+  if (!n) return fail(DCFR_ERR_INVALID_ARG, "NULL network");
+  *in_dim = n->in_dim;
+  *out_dim = n->out_dim;
+  *max_batch = n->max_batch;
+  return DCFR_OK;
+}
+
+// The network's forward pass on stream s, nothing synchronised: a solver
+// enqueues it between its kernels (and captures it in its graphs). y is the
+// network's own padded output buffer, valid until its next forward pass.
+int mlp_enqueue_forward(dcfr_mlp* n, const float* x, int m, cudaStream_t s, const float** y, int* ldy) {
+  int rc = batch_ok(n, m);
+  if (rc) return rc;
+  if ((rc = forward(n, x, m, pad128(m), s))) return rc;
+  *y = n->Y;
+  *ldy = n->nout[n->layers];
+  return DCFR_OK;
+}
+
+}  // namespace dcfr
 
 extern "C" {
 

@@ -125,6 +125,18 @@ struct FastTask {
   double a, b, c, d;  // as TermLane
 };
 
+// A depth-limited solve's leaf in one traversal: the leaf's ordinal, the
+// reach slot arriving at it and the value row (node id) it fills, and the
+// state entering the network (pot and effective stack in chips).
+struct LeafTask {
+  uint32_t leaf;
+  uint32_t slot;
+  uint32_t row;
+  uint32_t pad;
+  float pot;
+  float stack;
+};
+
 // A run of fast terminal tasks on one layout, processed by one block of the
 // warp terminal kernel (terminal_fast.cu): the block stages the layout once,
 // then its warps take the run's tasks one per warp.

@@ -54,9 +54,17 @@ struct WarpLayout {
   int L;
 };
 
+// Per-warp prefix storage needed by warp_terminal_task for layouts of up to
+// cstride elements: the prefixes (cstride + 1), then, 16-byte aligned, each
+// card's segment start prefix and total (52 x 2).
+__host__ __device__ constexpr size_t warp_prefix_entries(int cstride) {
+  return (((size_t)cstride + 1 + 1) & ~(size_t)1) + 2 * 52;
+}
+
 // One terminal task evaluated by one warp (all 32 lanes call it). row is
 // the warp's shared copy of the reach row (stride entries), G its prefix
-// array (L + 1 entries). The caller has checked the task's slot is live.
+// storage (warp_prefix_entries(cstride) entries, 16-byte aligned). The
+// caller has checked the task's slot is live.
 template <typename R>
 __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const FastTask& T, const WarpLayout& Y, R* row,
                                                    long long* G, int lane) {
@@ -66,6 +74,9 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
   const int L = Y.L;
   const int E = (((L + 31) >> 5) | 1);  // odd: conflict-free 8-byte strides
+  const uint32_t kind = T.kind;
+  const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
+  const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
   // 1. Row and its maximum.
   const R* src = A.reach + (size_t)T.slot * A.stride;
   R mx = 0;
@@ -88,6 +99,39 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   const double scale = pow2(S), inv = pow2(-S);
   const double pa = T.a * inv, pb = T.b * inv, pc = T.c * inv, pd = T.d * inv;
   __syncwarp();
+  if (fold) {
+    // A fold needs only the total T0 and each card's total (eval_fold,
+    // eval.rs:40-64): the same exact integer sums as the scan's, without it.
+    long long t0 = 0;
+    for (int k = lane; k < Y.seg[1]; k += 32) t0 += fixed(row[Y.cat[k]], scale);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) t0 += __shfl_xor_sync(0xffffffffu, t0, d);
+    for (int c = lane; c < 52; c += 32) {
+      long long tc = 0;
+      for (int k = Y.seg[1 + c]; k < Y.seg[2 + c]; k++) tc += fixed(row[Y.cat[k]], scale);
+      G[c] = tc;
+    }
+    __syncwarp();
+    R* out = A.vals + (size_t)T.row * A.stride;
+    for (int h = lane; h < hpp; h += 32) {
+      R v = 0;
+      if (h < np) {
+        const uint32_t w = Y.rec[h].w;
+        const int a = (int)(w & 0xFF), b = (int)((w >> 8) & 0xFF);
+        const uint16_t sm = Y.same[h];
+        const long long si = sm == 0xFFFF ? 0ll : fixed(row[sm], scale);
+        const long long F = t0 - G[a] - G[b] + si;
+        if constexpr (F64) {
+          v = pa * (double)F;
+        } else {
+          v = (scalar && t0 == 0) ? 0.0f : (float)(pa * (double)F);
+        }
+      }
+      out[h] = v;
+    }
+    __syncwarp();
+    return;
+  }
   // 2. Elements in layout order, lane sums, exclusive prefixes.
   const int k0 = lane * E, k1 = min(L, k0 + E);
   long long local = 0;
@@ -111,54 +155,39 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   const long long total = __shfl_sync(0xffffffffu, inc, 31);
   if (lane == 0) G[L] = total;
   __syncwarp();
+  // Each card's segment start prefix and total, once per task.
+  longlong2* cs = reinterpret_cast<longlong2*>(G + ((L + 2) & ~1));
+  for (int c = lane; c < 52; c += 32) {
+    const long long s0 = G[Y.seg[1 + c]];
+    cs[c] = make_longlong2(s0, G[Y.seg[2 + c]] - s0);
+  }
+  __syncwarp();
   // 3. Values in hand order.
   const long long T0 = G[Y.seg[1]];
   R* out = A.vals + (size_t)T.row * A.stride;
   R* fout = T.frow != NONE32 ? A.vals + (size_t)T.frow * A.stride : nullptr;
-  const uint32_t kind = T.kind;
-  const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
-  const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
   for (int h = lane; h < hpp; h += 32) {
     R v = 0, fv = 0;
     if (h < np) {
       const uint4 q = Y.rec[h];
       const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
-      const long long a0 = G[Y.seg[1 + a]], b0 = G[Y.seg[1 + b]];
-      const longlong2 ca = make_longlong2(a0, G[Y.seg[2 + a]] - a0);
-      const longlong2 cb = make_longlong2(b0, G[Y.seg[2 + b]] - b0);
+      const longlong2 ca = cs[a], cb = cs[b];
       const uint16_t sm = Y.same[h];
       const long long si = sm == 0xFFFF ? 0ll : fixed(row[sm], scale);
       const long long F = T0 - ca.y - cb.y + si;
-      if constexpr (F64) {
-        // Double rows: every value in double, no f32 rounding.
-        if (fold) {
-          v = pa * (double)F;
+      if (q.w >> 16) {
+        const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
+        const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
+        const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
+        const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
+        const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+        const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+        if constexpr (F64) {
+          // Double rows: every value in double, no f32 rounding.
+          double res = pa * (double)Wn + pb * (double)Lx;
+          if (T.c != 0.0) res += pc * (double)eq;
+          v = res;
         } else {
-          if (q.w >> 16) {
-            const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
-            const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
-            const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
-            const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
-            const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
-            double res = pa * (double)Wn + pb * (double)Lx;
-            if (T.c != 0.0) {
-              const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
-              res += pc * (double)eq;
-            }
-            v = res;
-          }
-          if (fout) fv = pd * (double)F;
-        }
-      } else if (fold) {
-        // eval_fold (eval.rs:40-64) returns zeros on a zero total.
-        v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
-      } else {
-        if (q.w >> 16) {
-          const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];
-          const long long Gaw = G[q.y & 0xFFFF], Gas = G[q.y >> 16];
-          const long long Gbw = G[q.z & 0xFFFF], Gbs = G[q.z >> 16];
-          const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
-          const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
           if (scalar) {
             v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
           } else {
@@ -166,12 +195,12 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
             res += pb * (double)Lx;
             v = (float)res;
           }
-          if (T.c != 0.0) {
-            const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
-            v += (float)(pc * (double)eq);
-          }
+          if (T.c != 0.0) v += (float)(pc * (double)eq);
         }
-        if (fout) fv = (float)(pd * (double)F);
+      }
+      if (fout) {
+        if constexpr (F64) fv = pd * (double)F;
+        else fv = (float)(pd * (double)F);
       }
     }
     out[h] = v;

@@ -36,6 +36,7 @@ EXPORTS = [
     "dcfr_batch_iteration_bytes",
     "dcfr_mlp_create", "dcfr_mlp_destroy", "dcfr_mlp_num_params", "dcfr_mlp_get_params", "dcfr_mlp_set_params",
     "dcfr_mlp_forward", "dcfr_mlp_gradients", "dcfr_mlp_train_step", "dcfr_gemm_bf16",
+    "dcfr_create_depth_limited", "dcfr_node_storage", "dcfr_write_node",
 ]
 
 
@@ -58,6 +59,10 @@ def lib():
         L.dcfr_synchronize.argtypes = [P]
         L.dcfr_exploitability.argtypes = [P, C.POINTER(C.c_double)]
         L.dcfr_exploitability_fp64.argtypes = [P, C.POINTER(C.c_double), P]
+        L.dcfr_create_depth_limited.argtypes = [C.POINTER(abi.Config), P, C.POINTER(P)]
+        L.dcfr_node_storage.argtypes = [P, P, C.c_size_t, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32)]
+        L.dcfr_write_node.argtypes = [P, P, C.c_size_t, P, P]
         L.dcfr_batch_create.argtypes = [P, C.c_int32, C.POINTER(P)]
         L.dcfr_batch_destroy.argtypes = [P]
         L.dcfr_batch_destroy.restype = None
@@ -221,6 +226,34 @@ class Solver:
         h = C.c_void_p()
         check(lib().dcfr_create(C.byref(config), C.byref(h)))
         return Solver(h)
+
+    @staticmethod
+    def new_depth_limited(config: abi.Config, net) -> "Solver":
+        """A flop solve cut at the turn deal, its leaves valued by `net`
+        (poker_trainer_b200.mlp.LeafNet, kept alive by the solver)."""
+        h = C.c_void_p()
+        check(lib().dcfr_create_depth_limited(C.byref(config), net._h, C.byref(h)))
+        s = Solver(h)
+        s._net = net
+        return s
+
+    def node_storage(self, path=()):
+        """(offset, actions, hands) of a decision node's block in the
+        reference storage layout."""
+        steps, n = abi.path_steps(path)
+        off = C.c_uint64()
+        na = C.c_int32()
+        nh = C.c_int32()
+        check(lib().dcfr_node_storage(self._h, steps, n, C.byref(off), C.byref(na), C.byref(nh)))
+        return off.value, na.value, nh.value
+
+    def write_node(self, path, regrets=None, sums=None):
+        """Overwrites a decision node's blocks ([actions][hands] arrays)."""
+        steps, n = abi.path_steps(path)
+        r = None if regrets is None else np.ascontiguousarray(regrets, np.float32)
+        sm = None if sums is None else np.ascontiguousarray(sums, np.float32)
+        check(lib().dcfr_write_node(self._h, steps, n, _ptr(r) if r is not None else None,
+                                    _ptr(sm) if sm is not None else None))
 
     @staticmethod
     def estimate(config: abi.Config) -> TreeStats:
