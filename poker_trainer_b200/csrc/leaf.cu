@@ -12,7 +12,9 @@
 //            the leaf's counterfactual value of traverser hand h is
 //              norm * factor * pot * sum_c [c not in h] EV_c(h) * m_c(h),
 //            the same sum a chance node forms over its children
-//            (cfr.rs:435-479), where m_c(h) is the opponent reach
+//            (cfr.rs:435-479), after a zero-sum correction of each card's
+//            network values (see leaf_values_kernel), where m_c(h) is the
+//            opponent reach
 //            compatible with h and c: with T the total, A[x] the reach of
 //            hands holding card x and R{x,y} the reach of combo {x,y},
 //              m_c(h) = T - A[h1] - A[h2] + R{h1,h2} - (A[c] - R{c,h1} - R{c,h2}).
@@ -80,48 +82,105 @@ __global__ void leaf_inputs_kernel(LeafArgs A, const LeafTask* __restrict__ task
   }
 }
 
-// Block per leaf task: the traverser's value row at the leaf.
+// Block per leaf task: the traverser's value row at the leaf. Before the
+// sum, each card's network values are made zero-sum (as the subgame is):
+// with S_q = sum over q's hands of r_q(h) m_c(h) EV_q,c(h) and M the joint
+// compatible mass, both sides are shifted by (S_p + S_o) / (2 M), so the
+// corrected values satisfy S_p + S_o = 0 exactly.
 __global__ void leaf_values_kernel(LeafArgs A, const LeafTask* __restrict__ tasks, const uint8_t* __restrict__ hc1_p,
                                    const uint8_t* __restrict__ hc2_p, const uint8_t* __restrict__ hc1_o,
                                    const uint8_t* __restrict__ hc2_o, int hp) {
   const LeafTask T = tasks[blockIdx.x];
   if (A.alive[T.slot] == 0) return;  // dead subtree (cfr.rs:267-274): row untouched
   const int p = A.p, o = p ^ 1;
-  __shared__ float R[DCFR_NUM_COMBOS];
-  __shared__ double Acard[52];
-  __shared__ double total;
-  const float* r = A.reach + (size_t)T.slot * A.stride;
-  for (int i = threadIdx.x; i < DCFR_NUM_COMBOS; i += blockDim.x) R[i] = 0.0f;
-  for (int i = threadIdx.x; i < 52; i += blockDim.x) Acard[i] = 0.0;
-  if (threadIdx.x == 0) total = 0.0;
+  __shared__ float R[2][DCFR_NUM_COMBOS];  // [0]: opponent, [1]: traverser, combo order
+  __shared__ double Acard[2][52];
+  __shared__ double total[2];
+  __shared__ double red[3][32];
+  __shared__ double shift[64];
+  const float* ro = A.reach + (size_t)T.slot * A.stride;
+  const float* rp = A.leaf_reach[p] + (size_t)T.leaf * A.stride;
+  for (int i = threadIdx.x; i < 2 * DCFR_NUM_COMBOS; i += blockDim.x) (&R[0][0])[i] = 0.0f;
+  for (int i = threadIdx.x; i < 104; i += blockDim.x) (&Acard[0][0])[i] = 0.0;
+  if (threadIdx.x < 2) total[threadIdx.x] = 0.0;
   __syncthreads();
-  const uint16_t* cbo = A.combos[o];
-  for (int j = threadIdx.x; j < A.n[o]; j += blockDim.x) {
-    const float v = r[j];
-    R[cbo[j]] = v;
-    if (v != 0.0f) {
-      atomicAdd(&Acard[hc1_o[j]], (double)v);
-      atomicAdd(&Acard[hc2_o[j]], (double)v);
-      atomicAdd(&total, (double)v);
+  for (int side = 0; side < 2; side++) {
+    const int q = side ? p : o;
+    const float* r = side ? rp : ro;
+    const uint8_t* c1 = side ? hc1_p : hc1_o;
+    const uint8_t* c2 = side ? hc2_p : hc2_o;
+    const uint16_t* cb = A.combos[q];
+    for (int j = threadIdx.x; j < A.n[q]; j += blockDim.x) {
+      const float v = r[j];
+      R[side][cb[j]] = v;
+      if (v != 0.0f) {
+        atomicAdd(&Acard[side][c1[j]], (double)v);
+        atomicAdd(&Acard[side][c2[j]], (double)v);
+        atomicAdd(&total[side], (double)v);
+      }
     }
   }
   __syncthreads();
-  const uint16_t* cbp = A.combos[p];
+  // m_c for a hand of one side: the other side's reach compatible with it and c.
+  auto mass = [&](int other, int h1, int h2, int ch, int c) -> double {
+    return total[other] - Acard[other][h1] - Acard[other][h2] + (double)R[other][ch] -
+           (Acard[other][c] - (double)R[other][combo_of(c, h1)] - (double)R[other][combo_of(c, h2)]);
+  };
+  const float* ybase = A.y + (size_t)T.leaf * A.nc * A.ldy;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int ci = 0; ci < A.nc; ci++) {
+    const int c = A.cards[ci];
+    const float* y = ybase + (size_t)ci * A.ldy;
+    double sp = 0.0, so = 0.0, mm = 0.0;
+    for (int h = threadIdx.x; h < A.n[p]; h += blockDim.x) {
+      const int h1 = hc1_p[h], h2 = hc2_p[h];
+      if (h1 == c || h2 == c) continue;
+      const int ch = A.combos[p][h];
+      const double w = (double)R[1][ch] * mass(0, h1, h2, ch, c);
+      sp += w * (double)y[(size_t)p * DCFR_NUM_COMBOS + ch];
+      mm += w;
+    }
+    for (int j = threadIdx.x; j < A.n[o]; j += blockDim.x) {
+      const int h1 = hc1_o[j], h2 = hc2_o[j];
+      if (h1 == c || h2 == c) continue;
+      const int ch = A.combos[o][j];
+      so += (double)R[0][ch] * mass(1, h1, h2, ch, c) * (double)y[(size_t)o * DCFR_NUM_COMBOS + ch];
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+      sp += __shfl_xor_sync(0xffffffffu, sp, d);
+      so += __shfl_xor_sync(0xffffffffu, so, d);
+      mm += __shfl_xor_sync(0xffffffffu, mm, d);
+    }
+    if (lane == 0) {
+      red[0][warp] = sp;
+      red[1][warp] = so;
+      red[2][warp] = mm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0, m = 0.0;
+      for (int w = 0; w < nw; w++) {
+        a += red[0][w];
+        b += red[1][w];
+        m += red[2][w];
+      }
+      shift[ci] = m > 0.0 ? 0.5 * (a + b) / m : 0.0;
+    }
+    __syncthreads();
+  }
   float* out = A.vals + (size_t)T.row * A.stride;
-  const float* y = A.y + (size_t)T.leaf * A.nc * A.ldy + (size_t)p * DCFR_NUM_COMBOS;
   const double scale = A.norm * (double)A.factor * (double)T.pot;
   for (int h = threadIdx.x; h < hp; h += blockDim.x) {
     float v = 0.0f;
     if (h < A.n[p]) {
       const int h1 = hc1_p[h], h2 = hc2_p[h];
-      const int ch = cbp[h];
-      const double base = total - Acard[h1] - Acard[h2] + (double)R[ch];
+      const int ch = A.combos[p][h];
       double acc = 0.0;
       for (int ci = 0; ci < A.nc; ci++) {
         const int c = A.cards[ci];
         if (c == h1 || c == h2) continue;
-        const double m = base - (Acard[c] - (double)R[combo_of(c, h1)] - (double)R[combo_of(c, h2)]);
-        acc += (double)y[(size_t)ci * A.ldy + ch] * m;
+        const double ev = (double)ybase[(size_t)ci * A.ldy + (size_t)p * DCFR_NUM_COMBOS + ch] - shift[ci];
+        acc += ev * mass(0, h1, h2, ch, c);
       }
       v = (float)(scale * acc);
     }

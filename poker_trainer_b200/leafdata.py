@@ -3,8 +3,10 @@ solver.
 
 A sample is one turn subgame of the flop workload: board Ks7s2d plus a turn
 card, a pot and effective stack reachable from the flop tree (both players
-put the same amount in on the flop), and both players' ranges narrowed from
-the flop ranges by seeded random per-class factors. The subgame is solved by
+put the same amount in on the flop: log-uniform pots from 600 to 12000
+chips, and all-in pots of 20000 with nothing behind 15% of the time), and
+both players' ranges narrowed from the flop ranges by seeded random
+per-class factors. The subgame is solved by
 libdcfr (fast precision, DCFR alpha 1.5 beta 0 gamma 2) to a target
 exploitability; the target of the sample is every hand's expected value
 under the average strategies, per player, in units of the pot.
@@ -60,7 +62,12 @@ def sample_state(rng, base0, base1):
     flop = abi.parse_cards(FLOP)
     turn = int(rng.choice([c for c in range(52) if c not in flop]))
     board = flop + [turn]
-    pot = int(rng.integers(600, 8001))
+    # Pots of the flop tree's leaves: both players put the same amount in on
+    # the flop, from nothing (600) to all in (20000, nothing behind).
+    if rng.random() < 0.15:
+        pot = 600 + 2 * 9700
+    else:
+        pot = int(round(600 * 20.0 ** rng.random()))
     stack = max(0, 9700 - (pot - 600) // 2)
     ranges = []
     classes = workloads.class_combos()

@@ -7,9 +7,10 @@ must equal the leaf formula evaluated here from the network's own outputs
 on inputs built the same way (both ranges in combo order with the dealt
 card's hands removed and scaled to a maximum of 1, board and card one-hot,
 pot and stack / 10000):
-  v[h] = norm * factor * pot * sum_c [c not in h] EV_c(h) * m_c(h),
-with m_c(h) the opponent's weight compatible with h and c and factor the
-chance node's 1/45."""
+  v[h] = norm * factor * pot * sum_c [c not in h] (EV_c(h) - s_c) * m_c(h),
+with m_c(h) the opponent's weight compatible with h and c, factor the
+chance node's 1/45, and s_c the zero-sum shift (S_p + S_o) / (2 M) of the
+card's network values."""
 import numpy as np
 import pytest
 
@@ -47,21 +48,27 @@ def test_leaf_values_follow_the_network(gpu):
             w.append(r)
         X.append(leafdata.encode(w[0], w[1], board + [c], pot, 0))
     Y = net.forward(torch.tensor(np.array(X), device="cuda")).cpu().numpy().astype(np.float64)
+    cp_all = [cc[hands[q][0]] for q in range(2)]
+    w_all = [hands[q][1].astype(np.float64) for q in range(2)]
+    compat = ~((cp_all[0][:, None, 0] == cp_all[1][None, :, 0]) | (cp_all[0][:, None, 0] == cp_all[1][None, :, 1]) |
+               (cp_all[0][:, None, 1] == cp_all[1][None, :, 0]) | (cp_all[0][:, None, 1] == cp_all[1][None, :, 1]))
     for p in range(2):
         o = 1 - p
         got = g.traverse(p, abi.MODE_AVERAGE, 1).astype(np.float64)
-        combos_p, _ = hands[p]
-        combos_o, wo = hands[o]
-        co = cc[combos_o]
-        exp = np.zeros(len(combos_p))
-        for i, cp in enumerate(combos_p):
-            h1, h2 = cc[cp]
-            compat = ~((co == h1) | (co == h2)).any(axis=1)
-            for k, c in enumerate(cards):
-                if c in (h1, h2):
-                    continue
-                m = float(wo[compat & ~(co == c).any(axis=1)].astype(np.float64).sum())
-                exp[i] += Y[k, p * 1326 + cp] * m
+        Cpo = compat if p == 0 else compat.T
+        exp = np.zeros(len(hands[p][0]))
+        for k, c in enumerate(cards):
+            vp = ~(cp_all[p] == c).any(axis=1)
+            vo = ~(cp_all[o] == c).any(axis=1)
+            mp = (Cpo[:, vo] @ w_all[o][vo]) * vp       # opponent mass of each traverser hand
+            mo = (Cpo.T[:, vp] @ w_all[p][vp]) * vo     # traverser mass of each opponent hand
+            evp = Y[k, p * 1326 + hands[p][0]]
+            evo = Y[k, o * 1326 + hands[o][0]]
+            sp = float((w_all[p] * mp * evp).sum())
+            so = float((w_all[o] * mo * evo).sum())
+            mm = float((w_all[p] * mp).sum())
+            shift = 0.5 * (sp + so) / mm if mm > 0 else 0.0
+            exp += (evp - shift) * mp
         exp *= norm * float(factor) * pot
         scale = float(np.max(np.abs(exp)))
         assert float(np.max(np.abs(got - exp))) <= 1e-4 * scale, (p, float(np.max(np.abs(got - exp))), scale)
