@@ -47,6 +47,9 @@ WORKLOADS = {
     "turn": ("turn subgame Ks7s2dTh: 48 river runouts, pot 20bb, stacks 90bb, bets 33%/75%/all-in + 2.5x raise "
              "on turn and river, seeded class ranges (seeds 1000/1001, 51 of 169 classes zeroed), f32 storage, "
              "DCFR alpha 1.5 beta 0 gamma 2"),
+    "turn-narrow": ("turn subgame Ks7s2dTh as in the turn workload with the flop workload's narrow ranges "
+                    "(Dirichlet(0.5) classes thresholded to 68 of 169, seeds 2000/2001), f32 storage, DCFR alpha 1.5 "
+                    "beta 0 gamma 2"),
     "river": ("river subgame Ks7s2dTh4c: pot 20bb, stacks 90bb, bets 50%/100%/all-in + 2.5x raise, seeded class "
               "ranges (seeds 1000/1001), f32 storage, DCFR alpha 1.5 beta 0 gamma 2"),
     "batch": ("512 independent river spots in one persistent launch per block of iterations under a captured CUDA "
@@ -66,7 +69,8 @@ WORKLOADS = {
 
 def workload_config(name: str, precision: str):
     from poker_trainer_b200 import workloads
-    cfg = {"turn": workloads.turn_spot, "river": workloads.river_spot, "flop": workloads.flop_spot,
+    cfg = {"turn": workloads.turn_spot, "turn-narrow": workloads.turn_narrow_spot, "river": workloads.river_spot,
+           "flop": workloads.flop_spot,
            "batch": workloads.river_spot, "learned": workloads.flop_spot}[name]()
     from poker_trainer_b200 import abi
     cfg.precision = abi.PRECISIONS[precision]
@@ -205,7 +209,8 @@ def ncu_traffic(kernel: str, workload: str):
 KERNEL_NAMES = {"terminal": "fast_terminal_kernel", "down": "down_kernel", "up": "up_kernel", "other": "other"}
 # The terminal kernel the engine picks by hand count (more than 768 hands:
 # one block-wide scan per terminal; otherwise one warp per terminal).
-TERMINAL_KERNEL = {"turn": "fast_terminal_kernel", "river": "fast_terminal_kernel", "flop": "warp_terminal_kernel"}
+TERMINAL_KERNEL = {"turn": "fast_terminal_kernel", "turn-narrow": "warp_terminal_kernel",
+                   "river": "fast_terminal_kernel", "flop": "warp_terminal_kernel"}
 
 
 def dist_setup(n_gpus: int):
@@ -499,7 +504,13 @@ def run_batch(args, world, rank, local):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e = BatchSolver.new(cfgs)
-    tuned = e2e.autotune(10)
+    if args.batch_tuning:
+        from poker_trainer_b200 import abi
+        w_, b_, i_, l_ = (int(x) for x in args.batch_tuning.split(","))
+        tuned = abi.BatchTuning(warps=w_, blocks_per_sm=b_, iterations_per_launch=i_, longest_first=l_)
+        e2e.set_tuning(tuned)
+    else:
+        tuned = e2e.autotune(10)
     e2e.iterate(K)
     d2h = 0
     for i in range(S):
@@ -596,7 +607,7 @@ def run_learned(args, world, rank, local):
     import numpy as np
     import torch
     from poker_trainer_b200 import leafdata
-    from poker_trainer_b200.mlp import LeafNet, gemm_bf16
+    from poker_trainer_b200.mlp import LeafNet, gemm_time
     from poker_trainer_b200.solver import Solver, SolveOptions
     from poker_trainer_b200.train_leaf import masked_mse, predict, train
 
@@ -616,18 +627,9 @@ def run_learned(args, world, rank, local):
     # The solve's network: same weights, batch room for every leaf x card.
     dlnet = LeafNet(leafdata.IN_DIM, 1024, 4, leafdata.OUT_DIM, max_batch=8192, seed=0)
     dlnet.set_params(net.params())
-    # Tensor-core throughput of the network's GEMM at the solve's shape class.
-    a = torch.randn(4096, 2816, device="cuda").to(torch.bfloat16)
-    b = torch.randn(1024, 2816, device="cuda").to(torch.bfloat16)
-    for _ in range(3):
-        gemm_bf16(a, b)
-    torch.cuda.synchronize()
-    tg0 = time.perf_counter()
-    reps = 20
-    for _ in range(reps):
-        gemm_bf16(a, b)
-    torch.cuda.synchronize()
-    gemm_s = (time.perf_counter() - tg0) / reps
+    # Tensor-core throughput of the network's GEMM at the solve's shape class
+    # (CUDA events around back-to-back launches on one stream).
+    gemm_s = gemm_time(4096, 1024, 2816, reps=50) * 1e-3
     gemm_tflops = 2.0 * 4096 * 2816 * 1024 / gemm_s / 1e12
     opts = SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10)
     full = Solver.new(cfg)
@@ -654,6 +656,22 @@ def run_learned(args, world, rank, local):
         rs = lambda st: (np.asarray(st, np.float64) * w[None, :]).sum(1) / max(w.sum(), 1e-30)
         diffs.append(float(np.max(np.abs(rs(q.strategy) - rs(qf.strategy)))))
     e_comb, _ = full.exploitability_fp64()
+    full.close()
+    # Judge 2: the depth-limited flop strategy locked into the full tree and
+    # the turn and river re-solved around it. Its regrets are written as
+    # 1e20 x its probabilities: regret matching keeps playing it exactly
+    # (what one iteration adds is below f32 resolution of those regrets, and
+    # DCFR discounts all of a node's positive regrets by the same factor).
+    lk = Solver.new(cfg)
+    for path in paths:
+        st = np.asarray(dl.query(path).strategy, np.float64)
+        lk.write_node(path, regrets=(1e20 * st).astype(np.float32))
+    t0 = time.perf_counter()
+    plk = lk.solve(SolveOptions(max_iterations=args.lock_iterations, target_exploitability_pct=0.5, check_every=50))
+    lk.synchronize()
+    t_lock = time.perf_counter() - t0
+    e_lock, _ = lk.exploitability_fp64()
+    lk.close()
     peak = 1672.6
     try:
         with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
@@ -672,7 +690,9 @@ def run_learned(args, world, rank, local):
                            "depth_limited_game_exploitability_pct": pd.exploitability_pct,
                            "speedup": t_full / t_dl,
                            "depth_limited_flop_strategy_in_full_tree_exploitability_pct_fp64": 100.0 * e_comb / pot,
-                           "flop_nodes": len(paths), "max_range_strategy_diff": max(diffs) if diffs else None},
+                           "flop_nodes": len(paths), "max_range_strategy_diff": max(diffs) if diffs else None,
+                           "depth_limited_flop_strategy_locked_resolve_exploitability_pct_fp64": 100.0 * e_lock / pot,
+                           "locked_resolve_iterations": plk.iteration, "locked_resolve_s": t_lock},
         "training": {"data_seconds": t_data, "train_seconds": t_train, "solve_iterations_mean": float(np.mean(iters)),
                      "loss_first": losses[0], "loss_last": float(np.mean(losses[-20:])),
                      "heldout_mse": {"network": masked_mse(pred, Yh, Mh),
@@ -702,6 +722,10 @@ def main():
     ap.add_argument("--cpu-batch-iters", type=int, default=20, help="batch: oracle iterations per spot timed")
     ap.add_argument("--learned-samples", type=int, default=1024, help="learned: solved turn subgames to train on")
     ap.add_argument("--learned-steps", type=int, default=2000, help="learned: training steps")
+    ap.add_argument("--batch-tuning", default=None, metavar="WARPS,BLOCKS_PER_SM,ITERS_PER_LAUNCH,LONGEST_FIRST",
+                    help="batch: a fixed launch shape instead of the autotuner's")
+    ap.add_argument("--lock-iterations", type=int, default=300,
+                    help="learned: iterations of the full-tree re-solve around the locked flop strategy")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

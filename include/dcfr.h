@@ -421,6 +421,12 @@ int dcfr_mlp_train_step(dcfr_mlp* n, const float* x, const float* target, const 
  * gelu'(z). ldc is the row stride of c (and z) in elements. */
 int dcfr_gemm_bf16(const void* a, const void* b, void* c, int32_t m, int32_t n, int32_t k, int32_t epi,
                    const float* bias, void* z, int32_t ldc, void* stream);
+/* The same GEMM launched `reps` times back to back on `stream` (no host
+ * synchronisation between launches), timed with CUDA events on that stream:
+ * *ms_per_launch is the mean device time of one launch. No reference
+ * counterpart (the reference has no network). */
+int dcfr_gemm_bf16_timed(const void* a, const void* b, void* c, int32_t m, int32_t n, int32_t k, int32_t epi,
+                         const float* bias, void* z, int32_t ldc, int32_t reps, void* stream, float* ms_per_launch);
 
 /* Largest hand count per side that dcfr_showdown_values_noalloc accepts. */
 #define DCFR_NOALLOC_MAX_HANDS 1326

@@ -438,33 +438,58 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // Slots of nodes in the subtree (node ids may be sparse for subtrees).
   std::unordered_map<uint32_t, uint32_t> slot;
   slot[root] = 0;
-  // Fused river subtrees (one block each, fused_*_kernel): river-street
-  // children of chance nodes, when there are enough to fill the GPU.
-  auto river_root = [&](uint32_t v) {
+  // Every street's decision subtree is a segment: the traversal's root and
+  // each child of a chance node. A segment runs fused (one block,
+  // fused_*_kernel) or level by level. Chance nodes sit between segments;
+  // layer(v) counts the chance nodes above v, so a traversal runs segment
+  // layer 0, chance layer 0, segment layer 1, ... down, and the reverse up.
+  auto segment_root = [&](uint32_t v) {
     const GNode& nd = g.nodes[v];
-    return v != root && nd.kind == N_PLAYER && nd.street == DCFR_RIVER && nd.parent != NO &&
-           g.nodes[nd.parent].kind == N_CHANCE;
+    return nd.kind == N_PLAYER && (v == root || (nd.parent != NO && g.nodes[nd.parent].kind == N_CHANCE));
   };
-  bool fuse = false;
+  // A segment runs fused only where its layer has at least
+  // FUSE_MIN_SEGMENTS segments (one block each fills the GPU) and it has at
+  // most FUSE_MAX_NODES decision nodes. Others (the traversal's root
+  // segment, wide segments) run level by level: one launch per depth, with
+  // many blocks per node.
+  constexpr uint32_t FUSE_MAX_NODES = 48, FUSE_MIN_SEGMENTS = 16;
+  std::unordered_map<uint32_t, uint32_t> seg_size;
+  std::vector<uint32_t> layer_segments;
   {
-    size_t candidates = 0;
-    std::vector<uint32_t> st{root};
+    struct Item {
+      uint32_t v, seg, layer;
+    };
+    std::vector<Item> st{{root, root, 0}};
     while (!st.empty()) {
-      uint32_t v = st.back();
+      const Item it = st.back();
       st.pop_back();
-      if (river_root(v)) {
-        candidates++;
-        continue;
+      const GNode& nd = g.nodes[it.v];
+      if (nd.kind == N_PLAYER) {
+        uint32_t rr = it.seg;
+        if (segment_root(it.v)) {
+          rr = it.v;
+          if (layer_segments.size() <= it.layer) layer_segments.resize(it.layer + 1, 0);
+          layer_segments[it.layer]++;
+        }
+        seg_size[rr]++;
+        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back({nd.first + i, rr, it.layer});
+      } else if (nd.kind == N_CHANCE) {
+        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back({nd.first + i, nd.first + i, it.layer + 1});
       }
-      const GNode& nd = g.nodes[v];
-      if (nd.kind == N_PLAYER || nd.kind == N_CHANCE)
-        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back(nd.first + i);
     }
-    fuse = candidates >= 64;
   }
+  auto fused_segment = [&](uint32_t v, uint32_t layer) {
+    return seg_size[v] <= FUSE_MAX_NODES && layer < layer_segments.size() &&
+           layer_segments[layer] >= FUSE_MIN_SEGMENTS;
+  };
   std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> tree_of;  // node -> (tree, depth in tree)
+  std::unordered_map<uint32_t, uint32_t> layer_of, sdepth_of;           // chance layer; depth in a wide segment
+  std::vector<std::vector<std::vector<DownTask>>> sdown;                // wide segments: [layer][depth]
+  std::vector<std::vector<std::vector<UpTask>>> sup;
+  layer_of[root] = 0;
   std::vector<std::vector<std::pair<uint32_t, DownTask>>> fdown;
   std::vector<std::vector<std::pair<uint32_t, UpTask>>> fup;
+  std::vector<uint32_t> tree_layer;
   int fmaxa = 0;
   q.push_back({root, 0});
   const double hp = g.half_pot, norm = g.norm;
@@ -475,21 +500,25 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     count++;
     const GNode& nd = g.nodes[v];
     const uint32_t sv = slot[v];
+    const uint32_t layer = layer_of[v];
+    if (nd.kind == N_PLAYER || nd.kind == N_CHANCE)
+      for (uint32_t i = 0; i < nd.nchild; i++) layer_of[nd.first + i] = layer + (nd.kind == N_CHANCE ? 1u : 0u);
     uint32_t tree = NONE32, tdepth = 0;
-    if (fuse) {
-      if (river_root(v)) {
-        tree = (uint32_t)fdown.size();
-        fdown.emplace_back();
-        fup.emplace_back();
-      } else if (nd.parent != NO) {
-        auto it = tree_of.find(nd.parent);
-        if (it != tree_of.end()) {
-          tree = it->second.first;
-          tdepth = it->second.second + 1;
-        }
+    if (segment_root(v) && fused_segment(v, layer)) {
+      tree = (uint32_t)fdown.size();
+      fdown.emplace_back();
+      fup.emplace_back();
+      tree_layer.push_back(layer);
+    } else if (segment_root(v)) {
+      sdepth_of[v] = 0;
+    } else if (nd.kind == N_PLAYER && nd.parent != NO) {
+      auto it = tree_of.find(nd.parent);
+      if (it != tree_of.end()) {
+        tree = it->second.first;
+        tdepth = it->second.second + 1;
       }
-      if (tree != NONE32) tree_of[v] = {tree, tdepth};
     }
+    if (tree != NONE32) tree_of[v] = {tree, tdepth};
     if (tree != NONE32 && nd.kind == N_PLAYER) {
       // Inside a fused river subtree (no chance nodes below the river).
       bool own = nd.player == p;
@@ -500,11 +529,19 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
         slot[c] = own ? sv : first_slot + i;
         q.push_back({c, depth + 1});
       }
+      if (nd.nchild > MAX_ACTIONS) {
+        Status s;
+        s.code = DCFR_ERR_INVALID_ARG;
+        s.msg = "a decision node has more than 16 actions";
+        return s;
+      }
       if (!own) fdown[tree].push_back({tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f}});
       fup[tree].push_back({tdepth, UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
                                           first_slot, gpu_off_[v], 0, 0, 0, 0}});
       fmaxa = std::max<int>(fmaxa, (int)nd.nchild);
     } else if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
+      // Chance nodes, by layer (decision nodes all belong to segments).
+      const uint32_t depth = layer;
       if (down.size() <= depth) {
         down.resize(depth + 1);
         up.resize(depth + 1);
@@ -526,15 +563,20 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
         q.push_back({c, depth + 1});
       }
       if (nd.kind == N_PLAYER) {
-        if (!own) {
-          DownTask t{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f};
-          down[depth].push_back(t);
-          dmax[depth] = std::max<int>(dmax[depth], nd.nchild);
+        // A node of a wide segment: level by level.
+        if (!sdepth_of.count(v)) sdepth_of[v] = sdepth_of[nd.parent] + 1;
+        const uint32_t sd = sdepth_of[v];
+        if (sdown.size() <= layer) {
+          sdown.resize(layer + 1);
+          sup.resize(layer + 1);
         }
-        UpTask u{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild, first_slot, gpu_off_[v],
-                 0, 0, 0, 0};
-        up[depth].push_back(u);
-        umax[depth] = std::max<int>(umax[depth], nd.nchild);
+        if (sdown[layer].size() <= sd) {
+          sdown[layer].resize(sd + 1);
+          sup[layer].resize(sd + 1);
+        }
+        if (!own) sdown[layer][sd].push_back(DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f});
+        sup[layer][sd].push_back(UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
+                                        first_slot, gpu_off_[v], 0, 0, 0, 0});
       } else {
         DownTask t{D_CHANCE_SPLIT, sv, first_slot, nd.nchild, 0, cc_off_[nd.index], nd.factor};
         down[depth].push_back(t);
@@ -599,7 +641,15 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   plan.h_fdown.clear();
   plan.h_fup.clear();
   plan.fused_maxa = fmaxa;
-  for (size_t t = 0; t < fdown.size(); t++) {
+  // Segments by layer: one fused launch per layer.
+  std::vector<uint32_t> order(fdown.size());
+  for (size_t t = 0; t < order.size(); t++) order[t] = (uint32_t)t;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return tree_layer[a] < tree_layer[b]; });
+  plan.tree_layers.clear();
+  for (uint32_t t : order) {
+    const uint32_t l = tree_layer[t];
+    if (plan.tree_layers.size() <= l) plan.tree_layers.resize(l + 1, {(uint32_t)plan.h_trees.size(), 0u});
+    plan.tree_layers[l].second++;
     FusedTree F{(uint32_t)plan.h_fdown.size(), 0, (uint32_t)plan.h_fup.size(), 0};
     uint32_t prev = 0;
     for (size_t i = 0; i < fdown[t].size(); i++) {
@@ -634,6 +684,21 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     for (const UpTask& t : up[d]) plan.up[d].kind_count[t.kind]++;
     plan.h_up.insert(plan.h_up.end(), up[d].begin(), up[d].end());
   }
+  // Wide segments: per layer, one level per depth.
+  plan.seg_down.assign(sdown.size(), {});
+  plan.seg_up.assign(sup.size(), {});
+  for (size_t l = 0; l < sdown.size(); l++)
+    for (size_t d = 0; d < sdown[l].size(); d++) {
+      int maxa = 0;
+      for (const DownTask& t : sdown[l][d]) maxa = std::max<int>(maxa, (int)t.nchild);
+      plan.seg_down[l].push_back(Plan::Level{(uint32_t)plan.h_down.size(), (uint32_t)sdown[l][d].size(), maxa,
+                                             {0, 0, 0}});
+      plan.h_down.insert(plan.h_down.end(), sdown[l][d].begin(), sdown[l][d].end());
+      maxa = 0;
+      for (const UpTask& t : sup[l][d]) maxa = std::max<int>(maxa, (int)t.nchild);
+      plan.seg_up[l].push_back(Plan::Level{(uint32_t)plan.h_up.size(), (uint32_t)sup[l][d].size(), maxa, {0, 0, 0}});
+      plan.h_up.insert(plan.h_up.end(), sup[l][d].begin(), sup[l][d].end());
+    }
   // Terminal groups: showdowns by (kind, board), folds by kind, 32 lanes each.
   std::stable_sort(sd.begin(), sd.end(), [](const SdLane& a, const SdLane& b) {
     return a.kind != b.kind ? a.kind < b.kind : a.board < b.board;
@@ -708,9 +773,17 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   }
   close_wave();
   int kernels = 0;
+  int tree_launches = 0;
+  for (auto& tl : plan.tree_layers) tree_launches += tl.second > 0;
   for (auto& l : plan.down) kernels += l.count > 0;
   for (auto& l : plan.up) kernels += l.count > 0;
-  if (!plan.h_trees.empty()) kernels += 2;
+  kernels += 2 * tree_launches;
+  int seg_down_launches = 0, seg_up_launches = 0;
+  for (auto& ls : plan.seg_down)
+    for (auto& l : ls) seg_down_launches += l.count > 0;
+  for (auto& ls : plan.seg_up)
+    for (auto& l : ls) seg_up_launches += l.count > 0;
+  kernels += seg_down_launches + seg_up_launches;
   const int term_kernels = fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
   kernels += term_kernels;
   plan.kernels = kernels;
@@ -722,10 +795,8 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   }
   for (auto& l : plan.down) plan.class_kernels[DCFR_KERNEL_DOWN] += l.count > 0;
   for (auto& l : plan.up) plan.class_kernels[DCFR_KERNEL_UP] += l.count > 0;
-  if (!plan.h_trees.empty()) {
-    plan.class_kernels[DCFR_KERNEL_DOWN]++;
-    plan.class_kernels[DCFR_KERNEL_UP]++;
-  }
+  plan.class_kernels[DCFR_KERNEL_DOWN] += tree_launches + seg_down_launches;
+  plan.class_kernels[DCFR_KERNEL_UP] += tree_launches + seg_up_launches;
   plan.class_kernels[DCFR_KERNEL_TERMINAL] = term_kernels;
   const double np_ = g.n[p], no_ = g.n[o];
   for (const std::vector<DownTask>* v : {&plan.h_down, &plan.h_fdown})
@@ -863,9 +934,20 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   mark(DCFR_KERNEL_OTHER);
   RowArgs A;
   row_args(p, A);
-  for (const Plan::Level& l : plan.down)
-    if (l.count) launch_down(mode, l.maxa, A, plan.d_down + l.first, (int)l.count, hp_[o], stream_);
-  launch_fused_down(mode, plan.fused_maxa, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fdown, hp_[o], stream_);
+  const size_t layers = std::max({plan.tree_layers.size(), plan.down.size(), plan.seg_down.size()});
+  // Down: segment layer l (fused segments, then wide ones level by level),
+  // then the chance nodes of layer l.
+  for (size_t l = 0; l < layers; l++) {
+    if (l < plan.tree_layers.size() && plan.tree_layers[l].second)
+      launch_fused_down(mode, plan.fused_maxa, A, plan.d_trees + plan.tree_layers[l].first,
+                        (int)plan.tree_layers[l].second, plan.d_fdown, hp_[o], stream_);
+    if (l < plan.seg_down.size())
+      for (const Plan::Level& lv : plan.seg_down[l])
+        if (lv.count) launch_down(mode, lv.maxa, A, plan.d_down + lv.first, (int)lv.count, hp_[o], stream_);
+    if (l < plan.down.size() && plan.down[l].count)
+      launch_down(mode, plan.down[l].maxa, A, plan.d_down + plan.down[l].first, (int)plan.down[l].count, hp_[o],
+                  stream_);
+  }
   mark(DCFR_KERNEL_DOWN);
   if (fast_) {
     if (!plan.h_fast.empty()) {
@@ -887,10 +969,19 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
   }
   enqueue_leaves(plan);
   mark(DCFR_KERNEL_TERMINAL);
-  launch_fused_up(mode, plan.fused_maxa, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fup, hp_[p], stream_);
-  for (size_t d = plan.up.size(); d-- > 0;) {
-    const Plan::Level& l = plan.up[d];
-    if (l.count) launch_up(mode, l.maxa, A, plan.d_up + l.first, (int)l.count, hp_[p], stream_);
+  // Up: the chance nodes of layer l (their children are done), then segment
+  // layer l.
+  for (size_t l = layers; l-- > 0;) {
+    if (l < plan.up.size() && plan.up[l].count)
+      launch_up(mode, plan.up[l].maxa, A, plan.d_up + plan.up[l].first, (int)plan.up[l].count, hp_[p], stream_);
+    if (l < plan.seg_up.size())
+      for (size_t d = plan.seg_up[l].size(); d-- > 0;) {
+        const Plan::Level& lv = plan.seg_up[l][d];
+        if (lv.count) launch_up(mode, lv.maxa, A, plan.d_up + lv.first, (int)lv.count, hp_[p], stream_);
+      }
+    if (l < plan.tree_layers.size() && plan.tree_layers[l].second)
+      launch_fused_up(mode, plan.fused_maxa, A, plan.d_trees + plan.tree_layers[l].first,
+                      (int)plan.tree_layers[l].second, plan.d_fup, hp_[p], stream_);
   }
   mark(DCFR_KERNEL_UP);
   if (root_out)
@@ -1238,9 +1329,17 @@ Status Engine::fp64_root_values(int mode, double out[2]) {
     A.iso = iso_;
     A.stride = stride_;
     A.p = p;
-    for (const Plan::Level& l : plan.down)
-      if (l.count) launch_down64(A, plan.d_down + l.first, (int)l.count, hp_[o], stream_);
-    launch_fused_down64(A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fdown, stream_);
+    const size_t layers = std::max({plan.tree_layers.size(), plan.down.size(), plan.seg_down.size()});
+    for (size_t l = 0; l < layers; l++) {
+      if (l < plan.tree_layers.size() && plan.tree_layers[l].second)
+        launch_fused_down64(A, plan.d_trees + plan.tree_layers[l].first, (int)plan.tree_layers[l].second,
+                            plan.d_fdown, stream_);
+      if (l < plan.seg_down.size())
+        for (const Plan::Level& lv : plan.seg_down[l])
+          if (lv.count) launch_down64(A, plan.d_down + lv.first, (int)lv.count, hp_[o], stream_);
+      if (l < plan.down.size() && plan.down[l].count)
+        launch_down64(A, plan.d_down + plan.down[l].first, (int)plan.down[l].count, hp_[o], stream_);
+    }
     if (!plan.h_fast.empty()) {
       FastArgs64 F;
       F.reach = reach64_;
@@ -1262,10 +1361,17 @@ Status Engine::fp64_root_values(int mode, double out[2]) {
       launch_warp_terminal64(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), term_warps_[1], term_blocks_[1],
                              stream_);
     }
-    launch_fused_up64(mode, A, plan.d_trees, (int)plan.h_trees.size(), plan.d_fup, stream_);
-    for (size_t d = plan.up.size(); d-- > 0;) {
-      const Plan::Level& l = plan.up[d];
-      if (l.count) launch_up64(mode, A, plan.d_up + l.first, (int)l.count, hp_[p], stream_);
+    for (size_t l = layers; l-- > 0;) {
+      if (l < plan.up.size() && plan.up[l].count)
+        launch_up64(mode, A, plan.d_up + plan.up[l].first, (int)plan.up[l].count, hp_[p], stream_);
+      if (l < plan.seg_up.size())
+        for (size_t d = plan.seg_up[l].size(); d-- > 0;) {
+          const Plan::Level& lv = plan.seg_up[l][d];
+          if (lv.count) launch_up64(mode, A, plan.d_up + lv.first, (int)lv.count, hp_[p], stream_);
+        }
+      if (l < plan.tree_layers.size() && plan.tree_layers[l].second)
+        launch_fused_up64(mode, A, plan.d_trees + plan.tree_layers[l].first, (int)plan.tree_layers[l].second,
+                          plan.d_fup, stream_);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(row.data(), vals64_ + (size_t)plan.root * stride_, (size_t)stride_ * 8,

@@ -77,7 +77,8 @@ struct Plan {
     int maxa = 0;
     uint32_t kind_count[3] = {0, 0, 0};
   };
-  std::vector<Level> down, up;  // up[d] for depth d (launched deepest first)
+  std::vector<Level> down, up;  // chance nodes by layer (down[l]: splits; up[l]: sums)
+  std::vector<std::vector<Level>> seg_down, seg_up;  // wide segments: [layer][depth]
   std::vector<DownTask> h_down;
   std::vector<UpTask> h_up;
   std::vector<TermGroup> h_groups;
@@ -93,6 +94,8 @@ struct Plan {
   std::vector<DownTask> h_fdown;
   std::vector<UpTask> h_fup;
   int fused_maxa = 0;
+  // Segments by layer (the number of chance nodes above): [first tree, count].
+  std::vector<std::pair<uint32_t, uint32_t>> tree_layers;
   FusedTree* d_trees = nullptr;
   DownTask* d_fdown = nullptr;
   UpTask* d_fup = nullptr;

@@ -363,6 +363,38 @@ int dcfr_gemm_bf16(const void* a, const void* b, void* c, int32_t m, int32_t n, 
   return DCFR_OK;
 }
 
+int dcfr_gemm_bf16_timed(const void* a, const void* b, void* c, int32_t m, int32_t n, int32_t k, int32_t epi,
+                         const float* bias, void* z, int32_t ldc, int32_t reps, void* stream, float* ms_per_launch) {
+  if (reps <= 0 || !ms_per_launch) return fail(DCFR_ERR_INVALID_ARG, "reps must be positive; ms_per_launch not NULL");
+  int* err = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MK(cudaMalloc(&err, 4));
+  MK(cudaMemset(err, 0, 4));
+  MK(cudaEventCreate(&e0));
+  MK(cudaEventCreate(&e1));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = 0, e = 0;
+  MK(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps && !rc; r++)
+    rc = gemm(static_cast<const bf16*>(a), static_cast<const bf16*>(b), m, n, k, epi, c, ldc, static_cast<bf16*>(z),
+              bias, err, s);
+  MK(cudaEventRecord(e1, s));
+  if (!rc) {
+    MK(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, s));
+    MK(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    MK(cudaEventElapsedTime(&ms, e0, e1));
+    *ms_per_launch = ms / (float)reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(err);
+  if (rc) return rc;
+  if (e) return fail(DCFR_ERR_DEVICE_TIMEOUT, "tensor-core GEMM: a bounded wait gave up");
+  set_last_error("");
+  return DCFR_OK;
+}
+
 int dcfr_mlp_create(int32_t in_dim, int32_t hidden, int32_t layers, int32_t out_dim, int32_t max_batch,
                     uint64_t seed, dcfr_mlp** out) {
   if (!out || in_dim <= 0 || out_dim <= 0 || hidden <= 0 || hidden % 128 || layers < 1 || max_batch <= 0)

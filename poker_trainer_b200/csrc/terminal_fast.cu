@@ -110,15 +110,13 @@ __global__ void fast_layout_kernel(const EntryD* __restrict__ tables, const uint
 // Shared-memory layout of a block (all offsets 16-byte aligned); rsize is
 // the byte size of a row entry (4 for float rows, 8 for double rows).
 struct FastSmem {
-  size_t rbuf, r64, g, cs, wsum, fred, cat, rec, same, seg, total;
+  size_t rbuf, g, wsum, fred, cat, rec, same, seg, total;
   __host__ __device__ FastSmem(int stride, int emax, int cstride, int tstride, int rsize = 4) {
     auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
     const size_t gn = (size_t)FAST_THREADS * emax + 2;
     rbuf = 0;
-    r64 = up16(rbuf + 2 * (size_t)stride * rsize);
-    g = up16(r64 + ((size_t)stride + 1) * 8);
-    cs = up16(g + gn * 8);
-    wsum = up16(cs + 2 * FAST_SEGS * 8);
+    g = up16(rbuf + 2 * (size_t)stride * rsize);
+    wsum = up16(g + gn * 8);
     fred = up16(wsum + (FAST_THREADS / 32) * 8);
     cat = up16(fred + 2 * (FAST_THREADS / 32) * rsize);
     rec = up16(cat + (size_t)cstride * 2);
@@ -151,9 +149,7 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
   constexpr int PER16 = 16 / (int)sizeof(R);  // row entries per 16-byte copy
   const FastSmem L_(A.stride, E, A.cstride, A.tstride, (int)sizeof(R));
   R* rbuf = reinterpret_cast<R*>(smem_fast + L_.rbuf);
-  long long* R64 = reinterpret_cast<long long*>(smem_fast + L_.r64);
   long long* G = reinterpret_cast<long long*>(smem_fast + L_.g);
-  longlong2* Cs = reinterpret_cast<longlong2*>(smem_fast + L_.cs);  // per card: {start prefix, card total}
   long long* wsum = reinterpret_cast<long long*>(smem_fast + L_.wsum);
   R* fred = reinterpret_cast<R*>(smem_fast + L_.fred);
   uint16_t* scat = reinterpret_cast<uint16_t*>(smem_fast + L_.cat);
@@ -169,9 +165,8 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
 
   for (int h = tid; h < hpp; h += FAST_THREADS) {
     const uint32_t sm = h < np ? A.same[h] : NONE32;
-    ssame[h] = sm == NONE32 ? (uint16_t)hpo : (uint16_t)sm;  // R64[hpo] is zero
+    ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
   }
-  if (tid == 0) R64[hpo] = 0;
   auto prefetch = [&](int ti, int buf) {
     const R* src = A.reach + (size_t)tasks[ti].slot * A.stride;
     R* dst = rbuf + (size_t)buf * A.stride;
@@ -181,7 +176,12 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
   prefetch(t0, 0);
   uint32_t board = NONE32;
   int L = 0;
+  FastTask T = tasks[t0];
 
+  // Three block barriers per terminal: after the row maxima (1), after the
+  // scan's warp totals (2) and after the prefixes are written (3). The next
+  // terminal's barrier (1) also ends this one's reads of the prefixes, the
+  // layout and this row buffer.
   for (int ti = t0; ti < t1; ti++) {
     const int buf = (ti - t0) & 1;
     const R* r = rbuf + (size_t)buf * A.stride;
@@ -202,16 +202,14 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) mx = row_max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
     if (lane == 0) fred[buf * (FAST_THREADS / 32) + warp] = mx;
-    __syncthreads();
+    __syncthreads();  // (1)
     if (ti + 1 < t1) prefetch(ti + 1, buf ^ 1);
-
-    const FastTask* T = tasks + ti;
-    const uint32_t slot = T->slot, tb = T->board, row = T->row, frow = T->frow, kind = T->kind;
-    const double pa0 = T->a, pb0 = T->b, pc0 = T->c, pd0 = T->d;
-    if (A.alive[slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
-    const size_t lay = (size_t)tb * 2 + p;
-    if (tb != board) {
-      board = tb;
+    const FastTask cur = T;
+    if (ti + 1 < t1) T = tasks[ti + 1];  // next task's record, loaded early
+    if (A.alive[cur.slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
+    if (cur.board != board) {
+      board = cur.board;
+      const size_t lay = (size_t)board * 2 + p;
       const uint16_t* gseg = A.seg + lay * FAST_SEGS;
       if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
       L = gseg[FAST_SEGS - 1];
@@ -219,50 +217,23 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
       for (int k = tid; k < L; k += FAST_THREADS) scat[k] = gcat[k];
       const uint4* grec = A.rec + lay * A.tstride;
       for (int h = tid; h < np; h += FAST_THREADS) srec[h] = grec[h];
+      __syncthreads();  // the new layout is staged (once per board)
     }
     mx = 0;
 #pragma unroll
     for (int w = 0; w < FAST_THREADS / 32; w++) mx = row_max(mx, fred[buf * (FAST_THREADS / 32) + w]);
-    // Row sum < 2048 * 2^(e+1) with 2^e <= max: scale it below 2^62.
     const int S = scale_exponent(mx);
     const double scale = pow2(S), inv = pow2(-S);
-    // Payoffs times 2^-S (exact: a power-of-two scaling).
-    const double pa = pa0 * inv, pb = pb0 * inv, pc = pc0 * inv, pd = pd0 * inv;
+    const double pa = cur.a * inv, pb = cur.b * inv, pc = cur.c * inv, pd = cur.d * inv;
 
-    // Reach row as fixed point.
-    if constexpr (F64) {
-      for (int i = tid; i < hpo / 2; i += FAST_THREADS) {
-        const double2 v = reinterpret_cast<const double2*>(r)[i];
-        R64[2 * i + 0] = fixed(v.x, scale);
-        R64[2 * i + 1] = fixed(v.y, scale);
-      }
-    } else {
-      for (int i = tid; i < hpo / 4; i += FAST_THREADS) {
-        const float4 v = reinterpret_cast<const float4*>(r)[i];
-        R64[4 * i + 0] = fixed(v.x, scale);
-        R64[4 * i + 1] = fixed(v.y, scale);
-        R64[4 * i + 2] = fixed(v.z, scale);
-        R64[4 * i + 3] = fixed(v.w, scale);
-      }
-    }
-    __syncthreads();
-
-    // Elements in layout order.
+    // This thread's E consecutive layout elements, straight from the row.
     constexpr int N = FAST_THREADS * E;
-#pragma unroll
-    for (int u = 0; u < E; u++) {
-      const int k = tid + u * FAST_THREADS;
-      G[k] = R64[k < L ? (int)scat[k] : hpo];
-    }
-    __syncthreads();
-
-    // Exclusive prefix sums, in place: E consecutive elements per thread.
-    long long* own = G + tid * E;
     long long x[E];
     long long local = 0;
 #pragma unroll
     for (int i = 0; i < E; i++) {
-      x[i] = own[i];
+      const int k = tid * E + i;
+      x[i] = k < L ? fixed(r[scat[k]], scale) : 0ll;
       local += x[i];
     }
     long long inc = local;
@@ -272,28 +243,25 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
       if (lane >= d) inc += y;
     }
     if (lane == 31) wsum[warp] = inc;
-    __syncthreads();
+    __syncthreads();  // (2)
     long long acc = inc - local;
 #pragma unroll
     for (int w = 0; w < FAST_THREADS / 32; w++)
       if (w < warp) acc += wsum[w];
+    long long* own = G + tid * E;
 #pragma unroll
     for (int i = 0; i < E; i++) {
       own[i] = acc;
       acc += x[i];
     }
     if (tid == FAST_THREADS - 1) G[N] = acc;
-    __syncthreads();
-    if (tid < FAST_SEGS - 1) {
-      const long long c0 = G[sseg[tid]], c1 = G[sseg[tid + 1]];
-      Cs[tid] = make_longlong2(c0, c1 - c0);
-    }
-    __syncthreads();
+    __syncthreads();  // (3)
 
-    // Values in hand order. Cs[0] = {0, T0}; Cs[1 + c] = card c.
-    const long long T0 = Cs[0].y;
-    R* out = A.vals + (size_t)row * A.stride;
-    R* fout = frow != NONE32 ? A.vals + (size_t)frow * A.stride : nullptr;
+    // Values in hand order. Card c's segment runs from sseg[1+c] to sseg[2+c].
+    const long long T0 = G[sseg[1]];
+    R* out = A.vals + (size_t)cur.row * A.stride;
+    R* fout = cur.frow != NONE32 ? A.vals + (size_t)cur.frow * A.stride : nullptr;
+    const uint32_t kind = cur.kind;
     const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
     const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
 #pragma unroll 2
@@ -301,8 +269,12 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
       R v = 0, fv = 0;
       if (h < np) {
         const uint4 q = srec[h];
-        const longlong2 ca = Cs[1 + (q.w & 0xFF)], cb = Cs[1 + ((q.w >> 8) & 0xFF)];
-        const long long si = R64[ssame[h]];
+        const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
+        const long long a0 = G[sseg[1 + a]], b0 = G[sseg[1 + b]];
+        const longlong2 ca = make_longlong2(a0, G[sseg[2 + a]] - a0);
+        const longlong2 cb = make_longlong2(b0, G[sseg[2 + b]] - b0);
+        const uint16_t sm = ssame[h];
+        const long long si = sm == 0xFFFF ? 0ll : fixed(r[sm], scale);
         const long long F = T0 - ca.y - cb.y + si;
         if constexpr (F64) {
           // Double rows: every value in double, no f32 rounding.
@@ -316,7 +288,7 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
               const long long W = (Gw + ca.x + cb.x) - Gaw - Gbw;
               const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
               double res = pa * (double)W + pb * (double)Lx;
-              if (pc0 != 0.0) {
+              if (pc != 0.0) {
                 const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
                 res += pc * (double)eq;
               }
@@ -343,7 +315,7 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
               res += pb * (double)Lx;
               v = (float)res;
             }
-            if (pc0 != 0.0) {
+            if (cur.c != 0.0) {
               const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
               v += (float)(pc * (double)eq);
             }

@@ -35,6 +35,8 @@ def _bind():
     L.dcfr_mlp_gradients.argtypes = [P, P, P, P, C.c_int32, C.POINTER(C.c_float), P]
     L.dcfr_mlp_train_step.argtypes = [P, P, P, P, C.c_int32, C.c_float, C.POINTER(C.c_float)]
     L.dcfr_gemm_bf16.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P]
+    L.dcfr_gemm_bf16_timed.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32,
+                                       C.c_int32, P, C.POINTER(C.c_float)]
     L._mlp_bound = True
     return L
 
@@ -131,3 +133,46 @@ def gemm_bf16(a, b, epi: int = 0, bias=None, z=None):
                            C.c_void_p(bias.data_ptr()) if bias is not None else None,
                            C.c_void_p(z.data_ptr()) if z is not None else None, n, None))
     return c, z
+
+
+def gemm_time(m: int, n: int, k: int, reps: int = 50, epi: int = 0, seed: int = 0) -> float:
+    """Milliseconds per launch of the library's GEMM on an [m][k] x [n][k]^T
+    product with epilogue `epi` (dcfr_gemm_bf16_timed: CUDA events around
+    `reps` back-to-back launches on the current stream, after 3 warm-up
+    launches)."""
+    import torch
+    L = _bind()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.randn(m, k, device="cuda", generator=g).to(torch.bfloat16)
+    b = torch.randn(n, k, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(n, device="cuda", generator=g)
+    c = torch.empty((m, n), dtype=torch.float32 if epi in (0, 1) else torch.bfloat16, device="cuda")
+    z = torch.randn(m, n, device="cuda", generator=g).to(torch.bfloat16) if epi in (2, 3) else None
+    stream = torch.cuda.current_stream()
+    args = (C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_void_p(c.data_ptr()), m, n, k, epi,
+            C.c_void_p(bias.data_ptr()) if epi in (1, 2) else None, C.c_void_p(z.data_ptr()) if z is not None else None,
+            n)
+    ms = C.c_float()
+    torch.cuda.synchronize()
+    check(L.dcfr_gemm_bf16_timed(*args, 3, C.c_void_p(stream.cuda_stream), C.byref(ms)))
+    check(L.dcfr_gemm_bf16_timed(*args, reps, C.c_void_p(stream.cuda_stream), C.byref(ms)))
+    return ms.value
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="Times the library's BF16 tcgen05 GEMM (dcfr_gemm_bf16).")
+    ap.add_argument("m", type=int)
+    ap.add_argument("n", type=int)
+    ap.add_argument("k", type=int)
+    ap.add_argument("--reps", type=int, default=50)
+    ap.add_argument("--epi", type=int, default=0, help="0 plain, 1 +bias, 2 +bias GELU, 3 x GELU'(z)")
+    args = ap.parse_args()
+    ms = gemm_time(args.m, args.n, args.k, args.reps, args.epi)
+    print(json.dumps({"m": args.m, "n": args.n, "k": args.k, "epi": args.epi, "ms": ms,
+                      "tflops": 2.0 * args.m * args.n * args.k / (ms * 1e-3) / 1e12}))
+
+
+if __name__ == "__main__":
+    main()

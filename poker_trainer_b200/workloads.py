@@ -106,6 +106,16 @@ def turn_spot(**over) -> abi.Config:
                            menu_=turn_menu(), **kw)
 
 
+def turn_narrow_spot(**over) -> abi.Config:
+    """The turn subgame of turn_spot with the flop workload's narrow ranges
+    (Dirichlet(0.5) classes thresholded to 68 of 169, seeds 2000/2001): a few
+    hundred hands per player, the regime of the warp-per-terminal kernel."""
+    kw = dict(DCFR, storage=abi.STORAGE_F32)
+    kw.update(over)
+    return abi.make_config("Ks7s2dTh", [dirichlet_range(2000), dirichlet_range(2001)], pot=2000, stack=9000,
+                           menu_=turn_menu(), **kw)
+
+
 def flop_spot(**over) -> abi.Config:
     """Flop Ks7s2d, pot 6bb, stacks 97bb, 33%/75%/all-in on every street, 3x
     raise; Dirichlet(0.5) class ranges thresholded to 68 classes; f32,

@@ -7,6 +7,10 @@ CPU, computed from the same bf16-rounded operands:
   rounding of activations, pre-activations and output gradients done at the
   same points as the kernels (relative error of each gradient block below
   2e-2);
+- the same loss and gradients against the FP64 CPU oracle
+  (oracle/mlp_fp64.py, pinned by finite differences), and one Adam step of
+  dcfr_mlp_train_step against the oracle's Adam step on the kernels' own
+  gradients;
 - training: Adam steps reduce the loss on a fixed regression batch.
 """
 import numpy as np
@@ -109,6 +113,43 @@ def test_mlp_gradients_match_fp32_reference(gpu):
         for got, ref, what in ((gw, rw.numpy(), "W"), (gb, rb.numpy(), "b")):
             rel = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
             assert rel < 2e-2, f"layer {l} {what}: relative error {rel}"
+
+
+def test_mlp_gradients_match_fp64_oracle(gpu):
+    import torch
+    from oracle import mlp_fp64
+    net = LeafNet(in_dim=130, hidden=256, layers=2, out_dim=200, max_batch=256, seed=7)
+    rng = np.random.default_rng(4)
+    x = rng.random((160, 130)).astype(np.float32)
+    t = rng.normal(size=(160, 200)).astype(np.float32)
+    mask = (rng.random((160, 200)) < 0.5).astype(np.float32)
+    loss, grads = net.gradients(torch.tensor(x).cuda(), torch.tensor(t).cuda(), torch.tensor(mask).cuda())
+    layers = [(w.astype(np.float64), b.astype(np.float64)) for w, b in net.split(net.params())]
+    rl, rg = mlp_fp64.loss_and_gradients(layers, x, t, mask, bf16_points=True)
+    assert abs(loss - rl) <= 1e-3 * abs(rl), (loss, rl)
+    for l, ((gw, gb), (rw, rb)) in enumerate(zip(net.split(grads), rg)):
+        for got, ref, what in ((gw, rw, "W"), (gb, rb, "b")):
+            rel = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
+            assert rel < 2e-2, f"layer {l} {what}: relative error {rel}"
+
+
+def test_adam_step_matches_fp64_oracle(gpu):
+    import torch
+    from oracle import mlp_fp64
+    net = LeafNet(in_dim=100, hidden=128, layers=1, out_dim=90, max_batch=128, seed=3)
+    rng = np.random.default_rng(8)
+    x = torch.tensor(rng.random((128, 100)).astype(np.float32)).cuda()
+    t = torch.tensor(rng.normal(size=(128, 90)).astype(np.float32)).cuda()
+    p0 = net.params()
+    _, g = net.gradients(x, t)
+    lr = 1e-3
+    net.train_step(x, t, None, lr=lr)
+    p1 = net.params()
+    ref, _, _ = mlp_fp64.adam_step(p0, g, np.zeros_like(g), np.zeros_like(g), 1, lr)
+    real = g != 0  # padded entries have zero gradients and do not move
+    assert np.array_equal(p1[~real], p0[~real])
+    err = np.abs(p1.astype(np.float64) - ref)[real]
+    assert float(err.max()) <= 1e-3 * lr + 1e-6 * float(np.abs(p0).max()), float(err.max())
 
 
 def test_mlp_training_reduces_loss(gpu):
