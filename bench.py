@@ -294,7 +294,9 @@ def run_ours(args, world, rank, local):
     g.synchronize()
     if sampler:
         sampler.begin()
-    prof = g.iterate_profiled(K)
+    # The timed region: K iterations as captured graph launches, CUDA events
+    # on the solver's stream around them (dcfr_last_iterate_ms).
+    g.iterate(K)
     g.synchronize()
     torch.cuda.synchronize()
     if sampler:
@@ -302,10 +304,11 @@ def run_ours(args, world, rank, local):
     barrier()
     launches = reduce(float(g.kernel_launches() - l0), "sum")
     clocks = sampler.close() if sampler else None
-    ms = reduce(prof["total_ms"], "max")
-    # Unprofiled graph launches of the same iterations, for comparison.
-    g.iterate(K)
-    plain_ms = reduce(g.last_iterate_ms(), "max")
+    ms = reduce(g.last_iterate_ms(), "max")
+    # The same iterations again with events between the kernel classes
+    # (the per-class breakdown and the roofline of the dominant class).
+    prof = g.iterate_profiled(K)
+    prof_ms = reduce(prof["total_ms"], "max")
     expl = g.exploitability()
     pot = float(cfg.root.pot)
     it_bytes = g.iteration_bytes()
@@ -349,8 +352,9 @@ def run_ours(args, world, rank, local):
             "l2": (f"inputs larger than L2: one iteration moves {working / 1e6:.0f} MB of rows and storage "
                    f"(> {L2_BYTES / 1e6:.0f} MB L2), no flush") if working > L2_BYTES else
                   "working set smaller than L2 (no flush; L2-resident figure)",
-            "timing": "CUDA events on the solver's stream around every kernel class, inside the captured "
-                      "iteration graph; max over ranks",
+            "timing": "value: CUDA events on the solver's stream around K captured-graph iterations, max over "
+                      "ranks; kernels and roofline: a second run of K iterations with events between the kernel "
+                      "classes inside the graph",
         },
         "clocks": clocks,
         "e2e": {"value": world * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
@@ -366,7 +370,7 @@ def run_ours(args, world, rank, local):
                                "achieved": it_bytes * (K / (ms / 1000.0)) / 1e9, "peak": peak, "unit": "GB/s",
                                "frac": it_bytes * (K / (ms / 1000.0)) / 1e9 / peak},
         "kernels": kernels,
-        "unprofiled_ms_per_step": plain_ms / K,
+        "profiled_ms_per_step": prof_ms / K,
         "exploitability_pct_after": 100.0 * expl / pot,
         "iterations_after": W + 2 * K,
         "cpu_baseline": cpu,

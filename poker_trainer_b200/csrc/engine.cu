@@ -721,22 +721,58 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       for (size_t k = i; k < j; k++) plan.h_lanes.push_back(folds[b][k]);
       plan.h_groups.push_back(G);
     }
-  // Fast precision: one task per terminal, showdowns by board, then folds.
-  plan.h_fast.clear();
+  // Fast precision: one task per terminal, grouped by layout. A fold below
+  // a river decision node is evaluated on its river board's layout: the
+  // opponent hands that layout leaves out hold a board card and have zero
+  // reach there, so every integer sum is the same as on the all-hands fold
+  // layout, and the board's folds interleave with its showdowns (blocks of
+  // the terminal kernels take contiguous task ranges; folds are cheaper).
+  // Other folds use the fold layout (index nboards).
+  const uint32_t nb = (uint32_t)g.boards.size();
+  std::unordered_map<uint32_t, uint32_t> seg_board;  // decision node -> river board below it
+  for (const SdLane& x : sd) {
+    uint32_t u = g.nodes[x.lane.row].parent;
+    while (u != NO && g.nodes[u].kind == N_PLAYER && !seg_board.count(u)) {
+      seg_board[u] = x.board;
+      u = g.nodes[u].parent;
+    }
+  }
+  std::vector<std::vector<FastTask>> by_sd(nb + 1), by_fold(nb + 1);
   for (const SdLane& x : sd) {
     const TermLane& L = x.lane;
-    plan.h_fast.push_back(FastTask{x.kind, x.board, L.slot, L.row, L.frow, {0, 0, 0}, L.a, L.b, L.c, L.d});
+    by_sd[x.board].push_back(FastTask{x.kind, x.board, L.slot, L.row, L.frow, {0, 0, 0}, L.a, L.b, L.c, L.d});
   }
   for (int b = 0; b < 2; b++)
-    for (const TermLane& L : folds[b])
-      plan.h_fast.push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, (uint32_t)g.boards.size(),
-                                     L.slot, L.row, NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
-  // Units of the warp terminal kernel: runs of at most TERM_UNIT tasks on
-  // one layout (h_fast is ordered by layout within each kind).
+    for (const TermLane& L : folds[b]) {
+      uint32_t layout = nb;
+      if (b)
+        for (uint32_t u = g.nodes[L.row].parent; u != NO && g.nodes[u].kind == N_PLAYER; u = g.nodes[u].parent) {
+          auto it = seg_board.find(u);
+          if (it != seg_board.end()) {
+            layout = it->second;
+            break;
+          }
+        }
+      by_fold[layout].push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, layout, L.slot, L.row,
+                                         NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
+    }
+  plan.h_fast.clear();
+  for (uint32_t l = 0; l <= nb; l++) {
+    const std::vector<FastTask>& S = by_sd[l];
+    const std::vector<FastTask>& F = by_fold[l];
+    // Interleave evenly: after k tasks, about k * |S| / (|S| + |F|) showdowns.
+    size_t i = 0, j = 0;
+    while (i < S.size() || j < F.size()) {
+      if (j >= F.size() || (i < S.size() && i * F.size() <= j * S.size())) plan.h_fast.push_back(S[i++]);
+      else plan.h_fast.push_back(F[j++]);
+    }
+  }
+  // Units of the warp terminal kernel: maximal runs of tasks on one layout
+  // (h_fast is ordered by layout).
   plan.h_units.clear();
   for (size_t i = 0; i < plan.h_fast.size();) {
     size_t j = i;
-    while (j < plan.h_fast.size() && j - i < (size_t)TERM_UNIT && plan.h_fast[j].board == plan.h_fast[i].board) j++;
+    while (j < plan.h_fast.size() && plan.h_fast[j].board == plan.h_fast[i].board) j++;
     plan.h_units.push_back(TermUnit{plan.h_fast[i].board, (uint32_t)i, (uint32_t)(j - i), 0});
     i = j;
   }
@@ -956,7 +992,8 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
       // Warp per terminal for short rows; one block-wide scan per terminal
       // for long rows, where a warp alone would scan too many elements.
       if (tstride_ <= WARP_TERMINAL_MAX_HANDS)
-        launch_warp_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), term_warps_[0], term_blocks_[0],
+        launch_warp_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
+                             term_warps_[0], term_blocks_[0],
                              stream_);
       else
         launch_fast_terminal(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, stream_);
@@ -1358,7 +1395,8 @@ Status Engine::fp64_root_values(int mode, double out[2]) {
       }
       F.stride = stride_;
       F.p = p;
-      launch_warp_terminal64(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), term_warps_[1], term_blocks_[1],
+      launch_warp_terminal64(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
+                               term_warps_[1], term_blocks_[1],
                              stream_);
     }
     for (size_t l = layers; l-- > 0;) {

@@ -42,9 +42,11 @@ void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstrid
                          uint16_t* cat, uint16_t* seg, uint4* rec, int cstride, cudaStream_t s);
 void launch_fast_terminal(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
 void launch_fast_terminal64(const FastArgs64& A, const FastTask* tasks, int ntasks, int max_blocks, cudaStream_t s);
-void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                          int warps,
                           int max_blocks, cudaStream_t s);
-void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
+void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                            int warps,
                             int max_blocks, cudaStream_t s);
 int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
 // FP64 best-response oracle kernels (br64.cu).

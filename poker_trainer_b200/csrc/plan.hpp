@@ -137,14 +137,13 @@ struct LeafTask {
   float stack;
 };
 
-// A run of fast terminal tasks on one layout, processed by one block of the
-// warp terminal kernel (terminal_fast.cu): the block stages the layout once,
-// then its warps take the run's tasks one per warp.
-constexpr int TERM_UNIT = 16;  // tasks per unit at most
 // Longest opponent hand list evaluated warp per terminal; longer lists use
 // the block-wide scan of fast_terminal_kernel (measured: the block kernel is
 // faster at 1128 hands, the warp kernel at 470).
 constexpr int WARP_TERMINAL_MAX_HANDS = 768;
+// A maximal run of fast terminal tasks on one layout. The warp terminal
+// kernel (terminal_fast.cu) stages a run's layout in shared memory once per
+// block whose task range meets the run.
 struct TermUnit {
   uint32_t layout;  // FastTask::board of every task in the run
   uint32_t first;   // first task

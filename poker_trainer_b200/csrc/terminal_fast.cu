@@ -130,7 +130,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Each block takes a contiguous range of the (board-sorted) task list. The
@@ -376,9 +375,12 @@ int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride) {
 //
 // The same fixed-point prefix sums as fast_terminal_kernel, but every
 // terminal is evaluated by one warp with no block barrier inside a task.
-// A block takes a unit (a run of tasks on one layout), stages that layout in
-// shared memory once, and its warps take the unit's tasks in turn. Per task
-// and warp:
+// Block b takes the contiguous task range [b N / G, (b+1) N / G) of the N
+// tasks (ordered by layout); its warps take the range's tasks in turn
+// (warp w: tasks w, w + W, ...). A unit is a maximal run of tasks on one
+// layout; the block stages a unit's layout in shared memory once, with a
+// block barrier only where its range crosses from one unit to the next.
+// Per task and warp:
 //   1. the reach row is copied to the warp's shared row (16-byte loads) and
 //      its maximum reduced across the warp, which fixes the scale 2^S;
 //   2. each lane converts E consecutive layout elements to fixed point,
@@ -389,8 +391,9 @@ int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride) {
 //      prefixes and the four card-segment bounds, exactly as
 //      fast_terminal_kernel does, and stores them coalesced.
 // Shared memory per block: the layout (elements, per-hand records,
-// identical-hand map, segment starts) and, per warp, one row and the
-// prefix array; the warp count W is a launch parameter.
+// identical-hand map, segment starts) and, per warp, two rows (the current
+// task's and the next one's, copied asynchronously) and the prefix array;
+// the warp count W is a launch parameter.
 struct WarpSmem {
   size_t same, cat, rec, seg, warp0, warp_bytes, row_bytes, total;
   __host__ __device__ WarpSmem(int stride, int cstride, int tstride, int rsize, int warps) {
@@ -401,14 +404,15 @@ struct WarpSmem {
     seg = up16(rec + (size_t)tstride * 16);
     warp0 = up16(seg + FAST_SEGS * 2);
     row_bytes = up16((size_t)stride * rsize);
-    warp_bytes = row_bytes + up16(warp_prefix_entries(cstride) * 8);
+    warp_bytes = 2 * row_bytes + up16(warp_prefix_entries(cstride) * 8);
     total = warp0 + (size_t)warps * warp_bytes;
   }
 };
 
 template <typename R>
 __global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
-                                                            const TermUnit* __restrict__ units, int nunits) {
+                                                            const TermUnit* __restrict__ units, int nunits,
+                                                            int ntasks) {
   extern __shared__ __align__(16) unsigned char smem_w[];
   const int W = (int)blockDim.x >> 5;
   const WarpSmem L_(A.stride, A.cstride, A.tstride, (int)sizeof(R), W);
@@ -418,7 +422,7 @@ __global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, cons
   uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_w + L_.seg);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   R* row = reinterpret_cast<R*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes);
-  long long* G = reinterpret_cast<long long*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes + L_.row_bytes);
+  long long* G = reinterpret_cast<long long*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes + 2 * L_.row_bytes);
 
   const int p = A.p;
   const int hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
@@ -427,7 +431,30 @@ __global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, cons
     ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
   }
 
-  for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+  const int t0 = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
+  const int t1 = (int)(((long long)(blockIdx.x + 1) * ntasks) / gridDim.x);
+  // The unit holding task t0: units tile [0, ntasks) in order.
+  int u = 0;
+  {
+    int hi = nunits - 1;
+    while (u < hi) {
+      const int mid = (u + hi) >> 1;
+      if ((int)(units[mid].first + units[mid].count) <= t0) u = mid + 1;
+      else hi = mid;
+    }
+  }
+  // Each warp double-buffers reach rows: the row of its next task is copied
+  // (cp.async) while the current task runs.
+  R* const row_b = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(row) + L_.row_bytes);
+  int buf = 0;
+  int next = t0 + warp;  // this warp's current task
+  bool live = false;
+  if (next < t1) {
+    live = A.alive[tasks[next].slot] != 0;
+    if (live) warp_row_prefetch<R>(A, tasks[next].slot, row, lane);
+  }
+  cp_async_commit();
+  for (; u < nunits && (int)units[u].first < t1; u++) {
     const TermUnit U = units[u];
     __syncthreads();  // the previous unit's warps are done with the layout
     const size_t lay = (size_t)U.layout * 2 + p;
@@ -440,10 +467,24 @@ __global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, cons
     for (int h = tid; h < np; h += blockDim.x) srec[h] = grec[h];
     __syncthreads();
     const WarpLayout Y{ssame, scat, srec, sseg, L};
-    for (uint32_t ti = U.first + warp; ti < U.first + U.count; ti += W) {
-      const FastTask T = tasks[ti];
-      if (A.alive[T.slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
-      warp_terminal_task<R>(A, T, Y, row, G, lane);
+    const int end = min(t1, (int)(U.first + U.count));
+    for (; next < end; next += W) {
+      // The following task's row (it may lie in a later unit: rows do not
+      // depend on the layout).
+      const int nx = next + W;
+      bool nlive = false;
+      if (nx < t1) {
+        const uint32_t ns = tasks[nx].slot;
+        nlive = A.alive[ns] != 0;
+        if (nlive) warp_row_prefetch<R>(A, ns, buf ? row : row_b, lane);
+      }
+      cp_async_commit();
+      cp_async_wait<1>();  // this task's row has landed
+      __syncwarp();
+      // Dead subtree (cfr.rs:267-274): row untouched.
+      if (live) warp_terminal_task<R, true>(A, tasks[next], Y, buf ? row_b : row, G, lane);
+      live = nlive;
+      buf ^= 1;
     }
   }
 }
@@ -479,21 +520,22 @@ int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max
 
 template <typename R>
 static void launch_warp_terminal_t(const FastArgsT<R>& A, const FastTask* tasks, const TermUnit* units, int nunits,
-                                   int warps, int max_blocks, cudaStream_t s) {
-  if (nunits <= 0) return;
-  const int blocks = nunits < max_blocks ? nunits : max_blocks;
+                                   int ntasks, int warps, int max_blocks, cudaStream_t s) {
+  if (nunits <= 0 || ntasks <= 0) return;
+  // At most one block per task: every block's range is non-empty.
+  const int blocks = ntasks < max_blocks ? ntasks : max_blocks;
   const size_t smem = warp_terminal_smem(A.stride, A.cstride, A.tstride, (int)sizeof(R), warps);
-  warp_terminal_kernel<R><<<blocks, warps * 32, smem, s>>>(A, tasks, units, nunits);
+  warp_terminal_kernel<R><<<blocks, warps * 32, smem, s>>>(A, tasks, units, nunits, ntasks);
 }
 
-void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
-                          int max_blocks, cudaStream_t s) {
-  launch_warp_terminal_t(A, tasks, units, nunits, warps, max_blocks, s);
+void launch_warp_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                          int warps, int max_blocks, cudaStream_t s) {
+  launch_warp_terminal_t(A, tasks, units, nunits, ntasks, warps, max_blocks, s);
 }
 
-void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int warps,
-                            int max_blocks, cudaStream_t s) {
-  launch_warp_terminal_t(A, tasks, units, nunits, warps, max_blocks, s);
+void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                            int warps, int max_blocks, cudaStream_t s) {
+  launch_warp_terminal_t(A, tasks, units, nunits, ntasks, warps, max_blocks, s);
 }
 
 void launch_fast_layouts(const EntryD* tables, const uint32_t* count, int tstride, int nboards, const uint8_t* hc1_0,

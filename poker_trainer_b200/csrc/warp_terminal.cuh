@@ -61,11 +61,31 @@ __host__ __device__ constexpr size_t warp_prefix_entries(int cstride) {
   return (((size_t)cstride + 1 + 1) & ~(size_t)1) + 2 * 52;
 }
 
+// Asynchronous copy (cp.async, 16-byte chunks through L2) of the reach row
+// of `slot` into the warp's shared row; it lands at a later cp.async wait.
+template <typename R>
+__device__ __forceinline__ void warp_row_prefetch(const FastArgsT<R>& A, uint32_t slot, R* row, int lane) {
+  constexpr int PER16 = 16 / (int)sizeof(R);
+  const int hpo = (A.p ^ 1) ? A.hp[1] : A.hp[0];
+  const char* src = reinterpret_cast<const char*>(A.reach + (size_t)slot * A.stride);
+  const uint32_t dst = (uint32_t)__cvta_generic_to_shared(row);
+  for (int i = lane; i < hpo / PER16; i += 32)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * (uint32_t)i), "l"(src + 16 * (size_t)i)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // One terminal task evaluated by one warp (all 32 lanes call it). row is
 // the warp's shared copy of the reach row (stride entries), G its prefix
 // storage (warp_prefix_entries(cstride) entries, 16-byte aligned). The
-// caller has checked the task's slot is live.
-template <typename R>
+// caller has checked the task's slot is live. With PRELOADED the row is
+// already in shared memory (warp_row_prefetch, waited for and synced);
+// otherwise it is loaded here.
+template <typename R, bool PRELOADED = false>
 __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const FastTask& T, const WarpLayout& Y, R* row,
                                                    long long* G, int lane) {
   constexpr bool F64 = sizeof(R) == 8;
@@ -82,14 +102,24 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   R mx = 0;
   if constexpr (F64) {
     for (int i = lane; i < hpo / PER16; i += 32) {
-      const double2 v = reinterpret_cast<const double2*>(src)[i];
-      reinterpret_cast<double2*>(row)[i] = v;
+      double2 v;
+      if constexpr (PRELOADED) {
+        v = reinterpret_cast<const double2*>(row)[i];
+      } else {
+        v = reinterpret_cast<const double2*>(src)[i];
+        reinterpret_cast<double2*>(row)[i] = v;
+      }
       mx = row_max(mx, row_max(v.x, v.y));
     }
   } else {
     for (int i = lane; i < hpo / PER16; i += 32) {
-      const float4 v = reinterpret_cast<const float4*>(src)[i];
-      reinterpret_cast<float4*>(row)[i] = v;
+      float4 v;
+      if constexpr (PRELOADED) {
+        v = reinterpret_cast<const float4*>(row)[i];
+      } else {
+        v = reinterpret_cast<const float4*>(src)[i];
+        reinterpret_cast<float4*>(row)[i] = v;
+      }
       mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
     }
   }
@@ -132,10 +162,22 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
     __syncwarp();
     return;
   }
-  // 2. Elements in layout order, lane sums, exclusive prefixes.
+  // 2. Elements in layout order, lane sums, exclusive prefixes (four
+  // independent elements per step; integer sums are order-free).
   const int k0 = lane * E, k1 = min(L, k0 + E);
   long long local = 0;
-  for (int k = k0; k < k1; k++) {
+  int k = k0;
+  for (; k + 4 <= k1; k += 4) {
+    const int c0 = Y.cat[k], c1 = Y.cat[k + 1], c2 = Y.cat[k + 2], c3 = Y.cat[k + 3];
+    const long long v0 = fixed(row[c0], scale), v1 = fixed(row[c1], scale);
+    const long long v2 = fixed(row[c2], scale), v3 = fixed(row[c3], scale);
+    G[k] = v0;
+    G[k + 1] = v1;
+    G[k + 2] = v2;
+    G[k + 3] = v3;
+    local += (v0 + v1) + (v2 + v3);
+  }
+  for (; k < k1; k++) {
     const long long v = fixed(row[Y.cat[k]], scale);
     G[k] = v;
     local += v;
@@ -147,7 +189,16 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
     if (lane >= d) inc += y;
   }
   long long acc = inc - local;
-  for (int k = k0; k < k1; k++) {
+  k = k0;
+  for (; k + 4 <= k1; k += 4) {
+    const long long v0 = G[k], v1 = G[k + 1], v2 = G[k + 2], v3 = G[k + 3];
+    G[k] = acc;
+    G[k + 1] = acc + v0;
+    G[k + 2] = acc + v0 + v1;
+    G[k + 3] = acc + v0 + v1 + v2;
+    acc += (v0 + v1) + (v2 + v3);
+  }
+  for (; k < k1; k++) {
     const long long v = G[k];
     G[k] = acc;
     acc += v;
@@ -166,8 +217,9 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   const long long T0 = G[Y.seg[1]];
   R* out = A.vals + (size_t)T.row * A.stride;
   R* fout = T.frow != NONE32 ? A.vals + (size_t)T.frow * A.stride : nullptr;
-  for (int h = lane; h < hpp; h += 32) {
-    R v = 0, fv = 0;
+  auto value = [&](int h, R& v, R& fv) {
+    v = 0;
+    fv = 0;
     if (h < np) {
       const uint4 q = Y.rec[h];
       const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
@@ -203,8 +255,25 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
         else fv = (float)(pd * (double)F);
       }
     }
-    out[h] = v;
-    if (fout) fout[h] = fv;
+  };
+  // Two hands per step: both hands' loads are issued before either store.
+  int h = lane;
+  for (; h + 32 < hpp; h += 64) {
+    R v0, f0, v1, f1;
+    value(h, v0, f0);
+    value(h + 32, v1, f1);
+    out[h] = v0;
+    out[h + 32] = v1;
+    if (fout) {
+      fout[h] = f0;
+      fout[h + 32] = f1;
+    }
+  }
+  if (h < hpp) {
+    R v0, f0;
+    value(h, v0, f0);
+    out[h] = v0;
+    if (fout) fout[h] = f0;
   }
   __syncwarp();  // the next task overwrites the row and the prefixes
 }

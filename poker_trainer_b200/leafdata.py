@@ -137,26 +137,43 @@ def equity_evs(state):
         g.close()
 
 
-def make_dataset(n: int, seed: int = 4000, target_pct=0.3, max_iterations=400, with_equity=False, base=None):
+def make_dataset(n: int, seed: int = 4000, target_pct=0.3, max_iterations=400, with_equity=False, base=None,
+                 workers: int = 4):
     """n solved samples: inputs [n][2706], targets [n][2652] (EV / pot),
-    masks [n][2652] and, optionally, the equity baseline's targets."""
+    masks [n][2652] and, optionally, the equity baseline's targets.
+
+    The states are drawn in order from the seed; `workers` host threads then
+    solve them concurrently, each with its own solver handle (its own CUDA
+    stream and graphs), so one subgame's host-side setup overlaps another's
+    GPU iterations. Every solve is deterministic, so the dataset does not
+    depend on `workers`."""
+    from concurrent.futures import ThreadPoolExecutor
     rng = np.random.default_rng(seed)
     if base is None:
         base = (workloads.dirichlet_range(2000), workloads.dirichlet_range(2001))
+    states = [sample_state(rng, *base) for _ in range(n)]
     X = np.zeros((n, IN_DIM), np.float32)
     Y = np.zeros((n, OUT_DIM), np.float32)
     M = np.zeros((n, OUT_DIM), np.float32)
     E = np.zeros((n, OUT_DIM), np.float32) if with_equity else None
-    iters = []
-    for i in range(n):
-        st = sample_state(rng, *base)
+    iters = [0] * n
+
+    def one(i):
+        st = states[i]
         board, pot, stack, ranges = st
         ev, mask, prog = solve_sample(st, target_pct, max_iterations)
         X[i] = encode(ranges[0], ranges[1], board, pot, stack)
         Y[i] = (ev / pot).reshape(-1)
         M[i] = mask.reshape(-1)
-        iters.append(prog.iteration)
+        iters[i] = prog.iteration
         if with_equity:
             eq, _ = equity_evs(st)
             E[i] = (eq / pot).reshape(-1)
+
+    if workers <= 1:
+        for i in range(n):
+            one(i)
+    else:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            list(ex.map(one, range(n)))
     return X, Y, M, E, iters
