@@ -545,6 +545,21 @@ def run_batch(args, world, rank, local):
     b.close()
     value = world * S * K / (ms / 1000.0)
     peak, peak_kind = measured_peak()
+    # The persistent kernel is the only kernel of the timed region: its
+    # algorithmic bytes per launch are every spot's B_iter times the
+    # iterations per launch; the committed ncu traffic is for 10 iterations
+    # per launch and scales with that count.
+    ipl = max(int(tuned.iterations_per_launch), 1)
+    n_launch = max(int(launches), 1)
+    per_launch_ms = ms / n_launch
+    per_launch_bytes = it_bytes * K / n_launch
+    traffic = ncu_traffic("batch_kernel", "batch")
+    roof = {"bound": "hbm", "kernel": "batch_kernel",
+            "achieved": per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0,
+            "peak": peak, "unit": "GB/s", "peak_kind": f"of {peak_kind}",
+            "traffic": traffic * ipl / 10.0 if traffic else None,
+            "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms}
+    roof["frac"] = roof["achieved"] / peak
     cpu = None
     if world == 1 and not args.no_cpu_baseline and rank == 0:
         L = oracle_lib()
@@ -575,10 +590,11 @@ def run_batch(args, world, rank, local):
                               "longest_first": tuned.longest_first, "candidates": tuned.candidates},
                    "l2": f"one iteration of all spots moves {it_bytes / 1e9:.2f} GB (> 126 MB L2), no flush"},
         "solve_ms": ms, "clocks": clocks,
-        "e2e": {"value": world * S * K / t_e2e, "unit": "spot-iterations/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": d2h / K,
+        "e2e": {"value": world * S * K / t_e2e, "unit": "spot-iterations/s",
+                "h2d_bytes_per_step": S * C.sizeof(cfgs[0]) / K, "d2h_bytes_per_step": d2h / K,
                 "what": "dcfr_batch_create + autotune + K iterations + every spot's storage read back, wall clock"},
         "gpu_launches": int(launches),
+        "roofline": roof,
         "iteration_roofline": {"bytes_per_iteration": it_bytes, "achieved": it_bytes * K / (ms / 1000.0) / 1e9,
                                "peak": peak, "unit": "GB/s", "frac": it_bytes * K / (ms / 1000.0) / 1e9 / peak,
                                "peak_kind": f"of {peak_kind}"},

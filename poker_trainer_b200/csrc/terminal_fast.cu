@@ -410,7 +410,7 @@ struct WarpSmem {
 };
 
 template <typename R>
-__global__ void __launch_bounds__(512) warp_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
+__global__ void __launch_bounds__(512, 1) warp_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
                                                             const TermUnit* __restrict__ units, int nunits,
                                                             int ntasks) {
   extern __shared__ __align__(16) unsigned char smem_w[];

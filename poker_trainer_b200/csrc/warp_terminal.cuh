@@ -24,6 +24,10 @@
 
 namespace dcfr {
 
+#ifndef WARP_TERMINAL_HANDS_PER_STEP
+#define WARP_TERMINAL_HANDS_PER_STEP 4
+#endif
+
 __device__ __forceinline__ double pow2(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
 // Fixed-point value of one reach entry: trunc(x * 2^S). Products are exact
@@ -256,20 +260,21 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
       }
     }
   };
-  // Two hands per step: both hands' loads are issued before either store.
+  // HU hands per step: all their loads are issued before any store.
+  constexpr int HU = WARP_TERMINAL_HANDS_PER_STEP;
   int h = lane;
-  for (; h + 32 < hpp; h += 64) {
-    R v0, f0, v1, f1;
-    value(h, v0, f0);
-    value(h + 32, v1, f1);
-    out[h] = v0;
-    out[h + 32] = v1;
+  for (; h + 32 * (HU - 1) < hpp; h += 32 * HU) {
+    R v[HU], f[HU];
+#pragma unroll
+    for (int u = 0; u < HU; u++) value(h + 32 * u, v[u], f[u]);
+#pragma unroll
+    for (int u = 0; u < HU; u++) out[h + 32 * u] = v[u];
     if (fout) {
-      fout[h] = f0;
-      fout[h + 32] = f1;
+#pragma unroll
+      for (int u = 0; u < HU; u++) fout[h + 32 * u] = f[u];
     }
   }
-  if (h < hpp) {
+  for (; h < hpp; h += 32) {
     R v0, f0;
     value(h, v0, f0);
     out[h] = v0;
