@@ -452,12 +452,18 @@ def run_flop(args, world, rank, local):
         "time_to_target": {"seconds": t_solve, "iterations": prog.iteration, "checks": len(checks),
                            "exploitability_pct": prog.exploitability_pct, "target_pct": 0.5,
                            "create_seconds": t_create,
+                           "end_to_end_seconds": t_create + t_solve,
                            "fp64_oracle_exploitability_pct": 100.0 * e64 / pot,
                            "f32_exploitability_pct": 100.0 * e32 / pot,
                            "fp64_vs_f32_rel": abs(e64 - e32) / max(abs(e64), 1e-30),
                            "speedup_vs_cpu": (cpu["time_to_target_s"] / t_solve) if cpu else None},
         "checks": checks,
         "clocks": clocks,
+        "e2e": {"value": prog.iteration / (t_create + t_solve), "unit": UNIT,
+                "h2d_bytes_per_step": C.sizeof(cfg) / max(prog.iteration, 1),
+                "d2h_bytes_per_step": 8.0 * len(checks) / max(prog.iteration, 1),
+                "what": "dcfr_create from the host config + dcfr_solve to the target with its exploitability "
+                        "checks (each reads one f64 back), wall clock; the iterations of the solve over that time"},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
                      "traffic": ncu_traffic(kname, "flop"), "bytes_per_launch": per_launch_bytes,

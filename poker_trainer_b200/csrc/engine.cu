@@ -435,8 +435,9 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   std::deque<std::pair<uint32_t, uint32_t>> q;  // node, depth
   std::vector<uint32_t> slot_of;                // by BFS discovery, indexed via map below
   std::vector<uint32_t> node_slot;
-  // Slots of nodes in the subtree (node ids may be sparse for subtrees).
-  std::unordered_map<uint32_t, uint32_t> slot;
+  // Per-node scratch, dense over node ids (a subtree plan touches a part).
+  const size_t NN = g.nodes.size();
+  std::vector<uint32_t> slot(NN, 0);
   slot[root] = 0;
   // Every street's decision subtree is a segment: the traversal's root and
   // each child of a chance node. A segment runs fused (one block,
@@ -453,7 +454,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // segment, wide segments) run level by level: one launch per depth, with
   // many blocks per node.
   constexpr uint32_t FUSE_MAX_NODES = 48, FUSE_MIN_SEGMENTS = 16;
-  std::unordered_map<uint32_t, uint32_t> seg_size;
+  std::vector<uint32_t> seg_size(NN, 0);
   std::vector<uint32_t> layer_segments;
   {
     struct Item {
@@ -482,8 +483,8 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     return seg_size[v] <= FUSE_MAX_NODES && layer < layer_segments.size() &&
            layer_segments[layer] >= FUSE_MIN_SEGMENTS;
   };
-  std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> tree_of;  // node -> (tree, depth in tree)
-  std::unordered_map<uint32_t, uint32_t> layer_of, sdepth_of;           // chance layer; depth in a wide segment
+  std::vector<uint32_t> tree_id(NN, NONE32), tree_depth(NN, 0);  // node -> fused tree and depth in it
+  std::vector<uint32_t> layer_of(NN, 0), sdepth_of(NN, NONE32);  // chance layer; depth in a wide segment
   std::vector<std::vector<std::vector<DownTask>>> sdown;                // wide segments: [layer][depth]
   std::vector<std::vector<std::vector<UpTask>>> sup;
   layer_of[root] = 0;
@@ -511,14 +512,14 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       tree_layer.push_back(layer);
     } else if (segment_root(v)) {
       sdepth_of[v] = 0;
-    } else if (nd.kind == N_PLAYER && nd.parent != NO) {
-      auto it = tree_of.find(nd.parent);
-      if (it != tree_of.end()) {
-        tree = it->second.first;
-        tdepth = it->second.second + 1;
-      }
+    } else if (nd.kind == N_PLAYER && nd.parent != NO && tree_id[nd.parent] != NONE32) {
+      tree = tree_id[nd.parent];
+      tdepth = tree_depth[nd.parent] + 1;
     }
-    if (tree != NONE32) tree_of[v] = {tree, tdepth};
+    if (tree != NONE32) {
+      tree_id[v] = tree;
+      tree_depth[v] = tdepth;
+    }
     if (tree != NONE32 && nd.kind == N_PLAYER) {
       // Inside a fused river subtree (no chance nodes below the river).
       bool own = nd.player == p;
@@ -564,7 +565,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       }
       if (nd.kind == N_PLAYER) {
         // A node of a wide segment: level by level.
-        if (!sdepth_of.count(v)) sdepth_of[v] = sdepth_of[nd.parent] + 1;
+        if (sdepth_of[v] == NONE32) sdepth_of[v] = sdepth_of[nd.parent] + 1;
         const uint32_t sd = sdepth_of[v];
         if (sdown.size() <= layer) {
           sdown.resize(layer + 1);
@@ -699,13 +700,15 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       plan.seg_up[l].push_back(Plan::Level{(uint32_t)plan.h_up.size(), (uint32_t)sup[l][d].size(), maxa, {0, 0, 0}});
       plan.h_up.insert(plan.h_up.end(), sup[l][d].begin(), sup[l][d].end());
     }
-  // Terminal groups: showdowns by (kind, board), folds by kind, 32 lanes each.
-  std::stable_sort(sd.begin(), sd.end(), [](const SdLane& a, const SdLane& b) {
-    return a.kind != b.kind ? a.kind < b.kind : a.board < b.board;
-  });
+  // Exact precision's terminal groups: showdowns by (kind, board), folds by
+  // kind, 32 lanes each (fast precision uses h_fast only).
+  if (!fast_)
+    std::stable_sort(sd.begin(), sd.end(), [](const SdLane& a, const SdLane& b) {
+      return a.kind != b.kind ? a.kind < b.kind : a.board < b.board;
+    });
   plan.h_groups.clear();
   plan.h_lanes.clear();
-  for (size_t i = 0; i < sd.size();) {
+  for (size_t i = 0; !fast_ && i < sd.size();) {
     size_t j = i;
     while (j < sd.size() && j - i < 32 && sd[j].kind == sd[i].kind && sd[j].board == sd[i].board) j++;
     TermGroup G{sd[i].kind, sd[i].board, (uint32_t)plan.h_lanes.size(), (uint32_t)(j - i)};
@@ -713,7 +716,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     plan.h_groups.push_back(G);
     i = j;
   }
-  for (int b = 0; b < 2; b++)
+  for (int b = 0; b < 2 && !fast_; b++)
     for (size_t i = 0; i < folds[b].size(); i += 32) {
       size_t j = std::min(folds[b].size(), i + 32);
       TermGroup G{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, 0, (uint32_t)plan.h_lanes.size(),
@@ -729,10 +732,10 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // the terminal kernels take contiguous task ranges; folds are cheaper).
   // Other folds use the fold layout (index nboards).
   const uint32_t nb = (uint32_t)g.boards.size();
-  std::unordered_map<uint32_t, uint32_t> seg_board;  // decision node -> river board below it
+  std::vector<uint32_t> seg_board(NN, NONE32);  // decision node -> river board below it
   for (const SdLane& x : sd) {
     uint32_t u = g.nodes[x.lane.row].parent;
-    while (u != NO && g.nodes[u].kind == N_PLAYER && !seg_board.count(u)) {
+    while (u != NO && g.nodes[u].kind == N_PLAYER && seg_board[u] == NONE32) {
       seg_board[u] = x.board;
       u = g.nodes[u].parent;
     }
@@ -746,13 +749,11 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     for (const TermLane& L : folds[b]) {
       uint32_t layout = nb;
       if (b)
-        for (uint32_t u = g.nodes[L.row].parent; u != NO && g.nodes[u].kind == N_PLAYER; u = g.nodes[u].parent) {
-          auto it = seg_board.find(u);
-          if (it != seg_board.end()) {
-            layout = it->second;
+        for (uint32_t u = g.nodes[L.row].parent; u != NO && g.nodes[u].kind == N_PLAYER; u = g.nodes[u].parent)
+          if (seg_board[u] != NONE32) {
+            layout = seg_board[u];
             break;
           }
-        }
       by_fold[layout].push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, layout, L.slot, L.row,
                                          NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
     }
@@ -843,8 +844,10 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     for (const UpTask& t : *v)
       plan.class_bytes[DCFR_KERNEL_UP] +=
           t.kind == U_OWN ? 4.0 * np_ * (3.0 * t.nchild + 1.0) : 4.0 * np_ * (t.nchild + 1.0);
-  for (const TermLane& L : plan.h_lanes)
-    plan.class_bytes[DCFR_KERNEL_TERMINAL] += 4.0 * (no_ + np_) + (L.frow != NONE32 ? 4.0 * np_ : 0.0);
+  // Per terminal: one reach row read, one value row written, and the paired
+  // fold's row.
+  for (const FastTask& t : plan.h_fast)
+    plan.class_bytes[DCFR_KERNEL_TERMINAL] += 4.0 * (no_ + np_) + (t.frow != NONE32 ? 4.0 * np_ : 0.0);
   return Status();
 }
 

@@ -6,8 +6,8 @@
 // A and B are row-major with K contiguous (both operands "K-major"). One CTA
 // computes a 128 x 128 tile of C:
 //   * warp 0, one thread: TMA loads of 128 x 64 tiles of A and B into a
-//     4-stage shared-memory ring (128-byte swizzle, the canonical K-major
-//     layout the tensor core reads);
+//     GEMM_STAGES-deep shared-memory ring (128-byte swizzle, the canonical
+//     K-major layout the tensor core reads);
 //   * warp 1, one thread: tcgen05.mma (M=128, N=128, K=16 per instruction,
 //     FP32 accumulator in tensor memory), a tcgen05.commit per stage frees
 //     the stage, a last commit marks the accumulator complete;
@@ -26,7 +26,16 @@
 
 namespace dcfr {
 
-constexpr int GEMM_BM = 128, GEMM_BN = 128, GEMM_BK = 64, GEMM_STAGES = 4, GEMM_THREADS = 128;
+// Two CTAs per SM (a 3-stage ring each, 97 KB of shared memory and 128
+// tensor-memory columns): one CTA's epilogue runs under the other's MMAs,
+// and a 4096 x 1024 output (256 tiles) fits the 148 SMs in one wave.
+#ifndef GEMM_STAGES_CFG
+#define GEMM_STAGES_CFG 3
+#endif
+#ifndef GEMM_CTAS_PER_SM
+#define GEMM_CTAS_PER_SM 2
+#endif
+constexpr int GEMM_BM = 128, GEMM_BN = 128, GEMM_BK = 64, GEMM_STAGES = GEMM_STAGES_CFG, GEMM_THREADS = 128;
 constexpr uint32_t GEMM_TILE_BYTES = GEMM_BM * GEMM_BK * 2;  // one 128 x 64 bf16 tile
 constexpr size_t GEMM_SMEM = 1024 + 2 * GEMM_STAGES * (size_t)GEMM_TILE_BYTES + 256;
 constexpr long long GEMM_WAIT_LIMIT = 1ll << 22;  // polls before a wait gives up (well over a second)
@@ -128,7 +137,7 @@ __device__ __forceinline__ float gelu_grad(float x) {
   return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
 }
 
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
+__global__ void __launch_bounds__(GEMM_THREADS, GEMM_CTAS_PER_SM)
     gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                         GemmArgs G) {
   extern __shared__ __align__(1024) unsigned char gemm_smem_raw[];
