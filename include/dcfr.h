@@ -415,6 +415,17 @@ int dcfr_mlp_gradients(dcfr_mlp* n, const float* x, const float* target, const f
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
 int dcfr_mlp_train_step(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t m, float lr,
                         float* loss);
+/* Data-parallel training (no reference counterpart): dcfr_mlp_backward
+ * leaves this batch's gradients in the device buffer that
+ * dcfr_mlp_gradients_device returns (flat padded layout, `count` floats;
+ * the network's stream is synchronised on return). The caller sums that
+ * buffer across ranks in place (an NCCL all-reduce) and synchronises, then
+ * dcfr_mlp_adam_step applies one Adam step to the buffer times gscale (1 /
+ * ranks for the mean). backward + adam_step(lr, 1) on one rank is
+ * dcfr_mlp_train_step. */
+int dcfr_mlp_backward(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t m, float* loss);
+int dcfr_mlp_gradients_device(dcfr_mlp* n, float** grads, uint64_t* count);
+int dcfr_mlp_adam_step(dcfr_mlp* n, float lr, float gscale);
 /* The tensor-core GEMM itself: c = epi(a[m][k] x b[n][k]^T) with a, b bf16
  * (k contiguous), m and n multiples of 128, k of 64; epi 0: c f32; 1: c f32
  * + bias[n]; 2: z bf16 = acc + bias, c bf16 = gelu(z); 3: c bf16 = acc *

@@ -196,10 +196,10 @@ __global__ void column_sums(const bf16* __restrict__ dY, int rows, int cols, flo
 // construction (pmask marks the real entries).
 __global__ void adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                      const uint8_t* __restrict__ pmask, size_t n, float lr, float b1, float b2, float eps, float c1,
-                     float c2) {
+                     float c2, float gscale) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !pmask[i]) return;
-  const float gi = g[i];
+  const float gi = g[i] * gscale;
   const float mi = b1 * m[i] + (1.0f - b1) * gi;
   const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
   m[i] = mi;
@@ -532,6 +532,17 @@ int dcfr_mlp_gradients(dcfr_mlp* n, const float* x, const float* target, const f
   return DCFR_OK;
 }
 
+// One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) on the
+// device gradients times gscale, then the bf16 weight copies.
+static int adam_step(dcfr_mlp* n, float lr, float gscale) {
+  n->step += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, (float)n->step), c2 = 1.0f - std::pow(b2, (float)n->step);
+  adam<<<blocks_for(n->nparams, 256), 256, 0, n->stream>>>(n->w, n->g, n->m, n->v, n->pmask, n->nparams, lr, b1, b2,
+                                                           1e-8f, c1, c2, gscale);
+  return refresh_bf16(n);
+}
+
 int dcfr_mlp_train_step(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t M, float lr,
                         float* loss) {
   if (!n || !x || !target) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
@@ -540,14 +551,42 @@ int dcfr_mlp_train_step(dcfr_mlp* n, const float* x, const float* target, const 
   const int Mp = pad128(M);
   if ((rc = forward(n, x, M, Mp))) return rc;
   if ((rc = backward(n, target, mask, M, Mp))) return rc;
-  n->step += 1;
-  const float b1 = 0.9f, b2 = 0.999f;
-  const float c1 = 1.0f - std::pow(b1, (float)n->step), c2 = 1.0f - std::pow(b2, (float)n->step);
-  adam<<<blocks_for(n->nparams, 256), 256, 0, n->stream>>>(n->w, n->g, n->m, n->v, n->pmask, n->nparams, lr, b1, b2,
-                                                           1e-8f, c1, c2);
-  if ((rc = refresh_bf16(n))) return rc;
+  if ((rc = adam_step(n, lr, 1.0f))) return rc;
   if ((rc = check_err(n))) return rc;
   if (loss) MK(cudaMemcpy(loss, n->loss, 4, cudaMemcpyDeviceToHost));
+  return DCFR_OK;
+}
+
+// Data-parallel training: the loss and gradients of this rank's batch stay
+// on the device (the stream is synchronised on return), the caller sums them
+// across ranks in place (an all-reduce on dcfr_mlp_gradients_device's
+// buffer), then dcfr_mlp_adam_step applies Adam to the sum times gscale.
+int dcfr_mlp_backward(dcfr_mlp* n, const float* x, const float* target, const float* mask, int32_t M, float* loss) {
+  if (!n || !x || !target) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  int rc = batch_ok(n, M);
+  if (rc) return rc;
+  const int Mp = pad128(M);
+  if ((rc = forward(n, x, M, Mp))) return rc;
+  if ((rc = backward(n, target, mask, M, Mp))) return rc;
+  if ((rc = check_err(n))) return rc;
+  if (loss) MK(cudaMemcpy(loss, n->loss, 4, cudaMemcpyDeviceToHost));
+  MK(cudaStreamSynchronize(n->stream));
+  return DCFR_OK;
+}
+
+int dcfr_mlp_gradients_device(dcfr_mlp* n, float** grads, uint64_t* count) {
+  if (!n || !grads || !count) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  *grads = n->g;
+  *count = n->nparams;
+  return DCFR_OK;
+}
+
+int dcfr_mlp_adam_step(dcfr_mlp* n, float lr, float gscale) {
+  if (!n) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  int rc = adam_step(n, lr, gscale);
+  if (rc) return rc;
+  if ((rc = check_err(n))) return rc;
+  MK(cudaStreamSynchronize(n->stream));
   return DCFR_OK;
 }
 

@@ -1,9 +1,10 @@
-"""One process per GPU for the benchmark's multi-GPU runs.
+"""One process per GPU for the multi-GPU runs.
 
 The solves shard by spot (independent units): every rank solves its own
-spots with no collective on the data path. torch.distributed is used only
-for the plumbing around the timed region: a barrier on entry and exit, and
-the maximum of the ranks' device times (the job time).
+spots with no collective on the data path; torch.distributed is used there
+only for the plumbing around the timed region (a barrier on entry and exit,
+and the maximum of the ranks' device times). The leaf network's
+data-parallel training sums gradients with an all-reduce (all_reduce_).
 """
 from __future__ import annotations
 
@@ -42,6 +43,17 @@ class Group:
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.SUM)
         return float(t.item())
+
+    def all_reduce_(self, t):
+        """Sum of the tensor t over ranks, in place (NCCL for CUDA tensors,
+        gloo for CPU ones); waits for the result."""
+        if self.dist is None:
+            return t
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        if t.is_cuda:
+            import torch
+            torch.cuda.synchronize(t.device)
+        return t
 
     def close(self):
         if self.dist is not None:

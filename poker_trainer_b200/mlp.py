@@ -34,6 +34,9 @@ def _bind():
     L.dcfr_mlp_forward.argtypes = [P, P, C.c_int32, P]
     L.dcfr_mlp_gradients.argtypes = [P, P, P, P, C.c_int32, C.POINTER(C.c_float), P]
     L.dcfr_mlp_train_step.argtypes = [P, P, P, P, C.c_int32, C.c_float, C.POINTER(C.c_float)]
+    L.dcfr_mlp_backward.argtypes = [P, P, P, P, C.c_int32, C.POINTER(C.c_float)]
+    L.dcfr_mlp_gradients_device.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+    L.dcfr_mlp_adam_step.argtypes = [P, C.c_float, C.c_float]
     L.dcfr_gemm_bf16.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P]
     L.dcfr_gemm_bf16_timed.argtypes = [P, P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32,
                                        C.c_int32, P, C.POINTER(C.c_float)]
@@ -108,6 +111,31 @@ class LeafNet:
                                        x.shape[0], C.byref(loss), g.ctypes.data_as(C.c_void_p)))
         return loss.value, g
 
+    def backward(self, x, target, mask=None) -> float:
+        """Loss of this batch; its gradients stay on the device
+        (grad_tensor), for a data-parallel sum before adam_step."""
+        import torch
+        torch.cuda.synchronize()
+        loss = C.c_float()
+        check(lib().dcfr_mlp_backward(self._h, _dev(x), _dev(target), _dev(mask) if mask is not None else None,
+                                      x.shape[0], C.byref(loss)))
+        return loss.value
+
+    def grad_tensor(self):
+        """The library's flat gradient buffer as a CUDA float32 torch tensor
+        (a view, no copy; valid while the network lives)."""
+        import torch
+        ptr = C.c_void_p()
+        n = C.c_uint64()
+        check(lib().dcfr_mlp_gradients_device(self._h, C.byref(ptr), C.byref(n)))
+        return torch.as_tensor(_DeviceArray(ptr.value, n.value), device="cuda")
+
+    def adam_step(self, lr: float = 1e-3, grad_scale: float = 1.0):
+        """One Adam step on the device gradients times grad_scale."""
+        import torch
+        torch.cuda.synchronize()
+        check(lib().dcfr_mlp_adam_step(self._h, lr, grad_scale))
+
     def train_step(self, x, target, mask=None, lr: float = 1e-3) -> float:
         import torch
         torch.cuda.synchronize()
@@ -115,6 +143,15 @@ class LeafNet:
         check(lib().dcfr_mlp_train_step(self._h, _dev(x), _dev(target), _dev(mask) if mask is not None else None,
                                         x.shape[0], lr, C.byref(loss)))
         return loss.value
+
+
+class _DeviceArray:
+    """A device buffer owned by the library, exposed to torch without a copy
+    (the CUDA array interface)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f4", "data": (ptr, False), "version": 3,
+                                         "strides": None, "stream": None}
 
 
 def gemm_bf16(a, b, epi: int = 0, bias=None, z=None):

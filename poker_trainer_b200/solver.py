@@ -35,7 +35,8 @@ EXPORTS = [
     "dcfr_batch_set_tuning", "dcfr_batch_last_iterate_ms", "dcfr_batch_iterations", "dcfr_batch_kernel_launches",
     "dcfr_batch_iteration_bytes",
     "dcfr_mlp_create", "dcfr_mlp_destroy", "dcfr_mlp_num_params", "dcfr_mlp_get_params", "dcfr_mlp_set_params",
-    "dcfr_mlp_forward", "dcfr_mlp_gradients", "dcfr_mlp_train_step", "dcfr_gemm_bf16", "dcfr_gemm_bf16_timed",
+    "dcfr_mlp_forward", "dcfr_mlp_gradients", "dcfr_mlp_train_step",
+    "dcfr_mlp_backward", "dcfr_mlp_gradients_device", "dcfr_mlp_adam_step", "dcfr_gemm_bf16", "dcfr_gemm_bf16_timed",
     "dcfr_create_depth_limited", "dcfr_node_storage", "dcfr_write_node",
 ]
 

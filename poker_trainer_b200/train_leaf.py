@@ -26,18 +26,39 @@ def masked_mse(pred: np.ndarray, y: np.ndarray, m: np.ndarray) -> float:
     return float((m * (pred - y) ** 2).sum() / max(m.sum(), 1.0))
 
 
-def train(X, Y, M, hidden=1024, layers=4, steps=2000, batch=256, lr=1e-3, seed=0, log=None):
+def train(X, Y, M, hidden=1024, layers=4, steps=2000, batch=256, lr=1e-3, seed=0, log=None, group=None, net=None,
+          device="cuda"):
+    """Adam on minibatches of `batch` samples. With a process group of R
+    ranks (poker_trainer_b200.dist.Group over NCCL) training is data-parallel:
+    every rank holds the same initial weights, draws its minibatch from its
+    own shard of the samples, and the ranks' gradients are summed by an
+    all-reduce on the library's device gradient buffer and averaged in the
+    Adam step, so the weights stay identical on every rank. `net` (default:
+    a new LeafNet) is anything with LeafNet's train_step, backward,
+    grad_tensor and adam_step on tensors of `device`."""
     import torch
+    world = group.world if group is not None else 1
+    rank = group.rank if group is not None else 0
     n = X.shape[0]
-    net = LeafNet(leafdata.IN_DIM, hidden, layers, leafdata.OUT_DIM, max_batch=batch, seed=seed)
-    Xd = torch.tensor(X, device="cuda")
-    Yd = torch.tensor(Y, device="cuda")
-    Md = torch.tensor(M, device="cuda")
-    rng = np.random.default_rng(seed)
+    if net is None:
+        net = LeafNet(leafdata.IN_DIM, hidden, layers, leafdata.OUT_DIM, max_batch=batch, seed=seed)
+    shard = np.arange(rank, n, world)
+    Xd = torch.tensor(X[shard], device=device)
+    Yd = torch.tensor(Y[shard], device=device)
+    Md = torch.tensor(M[shard], device=device)
+    ns = len(shard)
+    rng = np.random.default_rng(seed + 7919 * rank)
+    grads = net.grad_tensor() if world > 1 else None
     losses = []
     for s in range(steps):
-        idx = torch.tensor(rng.choice(n, min(batch, n), replace=False), device="cuda")
-        loss = net.train_step(Xd[idx].contiguous(), Yd[idx].contiguous(), Md[idx].contiguous(), lr=lr)
+        idx = torch.tensor(rng.choice(ns, min(batch, ns), replace=False), device=device)
+        xb, yb, mb = Xd[idx].contiguous(), Yd[idx].contiguous(), Md[idx].contiguous()
+        if world > 1:
+            loss = net.backward(xb, yb, mb)
+            group.all_reduce_(grads)
+            net.adam_step(lr, 1.0 / world)
+        else:
+            loss = net.train_step(xb, yb, mb, lr=lr)
         losses.append(loss)
         if log and (s % max(1, steps // 10) == 0 or s == steps - 1):
             log(s, loss)

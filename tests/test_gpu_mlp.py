@@ -166,3 +166,33 @@ def test_mlp_training_reduces_loss(gpu):
     assert last < 0.1 * first, (first, last)
     y = net.forward(xd).cpu()
     assert float(((y - t) ** 2).mean()) < 0.2 * first
+
+
+def test_data_parallel_entry_points(gpu):
+    """dcfr_mlp_backward + dcfr_mlp_adam_step(lr, 1) is dcfr_mlp_train_step,
+    bit for bit; the device gradient buffer (a torch view, as NCCL sees it)
+    holds the gradients dcfr_mlp_gradients returns; scaling the buffer by 2
+    and stepping with grad_scale 0.5 is the same step again (the
+    data-parallel mean over two equal ranks)."""
+    import torch
+    rng = np.random.default_rng(12)
+    x = torch.tensor(rng.random((128, 150)).astype(np.float32)).cuda()
+    t = torch.tensor(rng.normal(size=(128, 100)).astype(np.float32)).cuda()
+    a = LeafNet(in_dim=150, hidden=128, layers=2, out_dim=100, max_batch=128, seed=4)
+    b = LeafNet(in_dim=150, hidden=128, layers=2, out_dim=100, max_batch=128, seed=4)
+    c = LeafNet(in_dim=150, hidden=128, layers=2, out_dim=100, max_batch=128, seed=4)
+    _, g_host = a.gradients(x, t)
+    la = a.train_step(x, t, None, lr=1e-3)
+    lb = b.backward(x, t)
+    gv = b.grad_tensor()
+    assert gv.is_cuda and gv.numel() == b.num_params
+    assert np.array_equal(gv.cpu().numpy(), g_host)
+    b.adam_step(1e-3, 1.0)
+    assert la == lb
+    assert np.array_equal(a.params(), b.params())
+    c.backward(x, t)
+    gc = c.grad_tensor()
+    gc.mul_(2.0)
+    torch.cuda.synchronize()
+    c.adam_step(1e-3, 0.5)
+    assert np.array_equal(a.params(), c.params())
