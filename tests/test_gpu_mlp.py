@@ -188,7 +188,9 @@ def test_data_parallel_entry_points(gpu):
     assert gv.is_cuda and gv.numel() == b.num_params
     assert np.array_equal(gv.cpu().numpy(), g_host)
     b.adam_step(1e-3, 1.0)
-    assert la == lb
+    # The loss scalar is reduced with float atomics (order-dependent in the
+    # last bits); the gradients and the weights are not.
+    assert abs(la - lb) <= 1e-5 * abs(la)
     assert np.array_equal(a.params(), b.params())
     c.backward(x, t)
     gc = c.grad_tensor()
