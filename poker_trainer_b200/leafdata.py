@@ -138,7 +138,7 @@ def equity_evs(state):
 
 
 def make_dataset(n: int, seed: int = 4000, target_pct=0.3, max_iterations=400, with_equity=False, base=None,
-                 workers: int = 4):
+                 workers: int = 4, part=(0, 1)):
     """n solved samples: inputs [n][2706], targets [n][2652] (EV / pot),
     masks [n][2652] and, optionally, the equity baseline's targets.
 
@@ -146,12 +146,15 @@ def make_dataset(n: int, seed: int = 4000, target_pct=0.3, max_iterations=400, w
     solve them concurrently, each with its own solver handle (its own CUDA
     stream and graphs), so one subgame's host-side setup overlaps another's
     GPU iterations. Every solve is deterministic, so the dataset does not
-    depend on `workers`."""
+    depend on `workers`. part = (r, R) solves and returns only the samples
+    r, r + R, ... (rank r of R data-parallel ranks)."""
     from concurrent.futures import ThreadPoolExecutor
     rng = np.random.default_rng(seed)
     if base is None:
         base = (workloads.dirichlet_range(2000), workloads.dirichlet_range(2001))
     states = [sample_state(rng, *base) for _ in range(n)]
+    states = states[part[0]::part[1]]
+    n = len(states)
     X = np.zeros((n, IN_DIM), np.float32)
     Y = np.zeros((n, OUT_DIM), np.float32)
     M = np.zeros((n, OUT_DIM), np.float32)

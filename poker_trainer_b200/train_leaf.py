@@ -2,6 +2,11 @@
 
     python -m poker_trainer_b200.train_leaf [--samples N] [--hidden 1024]
         [--layers 4] [--steps S] [--out weights.npz]
+    torchrun --nproc-per-node R -m poker_trainer_b200.train_leaf ...
+
+Under torchrun every rank solves its share of the subgames and training is
+data-parallel (train: an NCCL all-reduce of the gradients each step); rank 0
+reports.
 
 Generation (leafdata.make_dataset) and training both run on the GPU: the
 subgames through libdcfr's solver, the network through libdcfr's BF16
@@ -14,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
 
 import numpy as np
@@ -27,7 +33,7 @@ def masked_mse(pred: np.ndarray, y: np.ndarray, m: np.ndarray) -> float:
 
 
 def train(X, Y, M, hidden=1024, layers=4, steps=2000, batch=256, lr=1e-3, seed=0, log=None, group=None, net=None,
-          device="cuda"):
+          device="cuda", local=False):
     """Adam on minibatches of `batch` samples. With a process group of R
     ranks (poker_trainer_b200.dist.Group over NCCL) training is data-parallel:
     every rank holds the same initial weights, draws its minibatch from its
@@ -35,14 +41,15 @@ def train(X, Y, M, hidden=1024, layers=4, steps=2000, batch=256, lr=1e-3, seed=0
     all-reduce on the library's device gradient buffer and averaged in the
     Adam step, so the weights stay identical on every rank. `net` (default:
     a new LeafNet) is anything with LeafNet's train_step, backward,
-    grad_tensor and adam_step on tensors of `device`."""
+    grad_tensor and adam_step on tensors of `device`. local: X, Y, M are
+    already this rank's shard."""
     import torch
     world = group.world if group is not None else 1
     rank = group.rank if group is not None else 0
     n = X.shape[0]
     if net is None:
         net = LeafNet(leafdata.IN_DIM, hidden, layers, leafdata.OUT_DIM, max_batch=batch, seed=seed)
-    shard = np.arange(rank, n, world)
+    shard = np.arange(n) if local else np.arange(rank, n, world)
     Xd = torch.tensor(X[shard], device=device)
     Yd = torch.tensor(Y[shard], device=device)
     Md = torch.tensor(M[shard], device=device)
@@ -86,19 +93,29 @@ def main():
     ap.add_argument("--max-iterations", type=int, default=400)
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
+    import torch
+    from .dist import Group
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    group = Group("nccl", torch.device("cuda", local_rank))
     t0 = time.perf_counter()
     X, Y, M, _, iters = leafdata.make_dataset(args.samples, seed=4000, target_pct=args.target_pct,
-                                              max_iterations=args.max_iterations)
-    Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(args.heldout, seed=5000, target_pct=args.target_pct,
-                                              max_iterations=args.max_iterations, with_equity=True)
-    t_data = time.perf_counter() - t0
+                                              max_iterations=args.max_iterations, part=(group.rank, group.world))
+    if group.rank == 0:
+        Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(args.heldout, seed=5000, target_pct=args.target_pct,
+                                                  max_iterations=args.max_iterations, with_equity=True)
+    t_data = group.reduce(time.perf_counter() - t0, "max")
     t0 = time.perf_counter()
-    net, losses = train(X, Y, M, args.hidden, args.layers, args.steps, args.batch, args.lr)
-    t_train = time.perf_counter() - t0
+    net, losses = train(X, Y, M, args.hidden, args.layers, args.steps, args.batch, args.lr, group=group, local=True)
+    t_train = group.reduce(time.perf_counter() - t0, "max")
+    group.close()
+    if group.rank != 0:
+        return
     pred = predict(net, Xh)
     mean = (Y * M).sum(0) / np.maximum(M.sum(0), 1.0)
     line = {
-        "samples": args.samples, "heldout": args.heldout, "solve_iterations_mean": float(np.mean(iters)),
+        "samples": args.samples, "heldout": args.heldout, "ranks": group.world,
+        "solve_iterations_mean": float(np.mean(iters)),
         "data_seconds": t_data, "train_seconds": t_train, "steps": args.steps,
         "network": {"hidden": args.hidden, "layers": args.layers, "params": net.num_params},
         "train_loss_first": losses[0], "train_loss_last": float(np.mean(losses[-20:])),
