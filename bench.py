@@ -404,11 +404,13 @@ def run_flop(args, world, rank, local):
     torch.cuda.synchronize()
     if sampler:
         sampler.begin()
+    l0 = g.kernel_launches()
     t0 = time.perf_counter()
     prog = g.solve(SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10),
                    on_progress=lambda pr: checks.append((pr.iteration, pr.exploitability_pct)) or True)
     g.synchronize()
     t_solve = time.perf_counter() - t0
+    solve_launches = g.kernel_launches() - l0
     if sampler:
         sampler.end()
     clocks = sampler.close() if sampler else None
@@ -459,6 +461,7 @@ def run_flop(args, world, rank, local):
                            "speedup_vs_cpu": (cpu["time_to_target_s"] / t_solve) if cpu else None},
         "checks": checks,
         "clocks": clocks,
+        "gpu_launches": int(solve_launches),
         "e2e": {"value": prog.iteration / (t_create + t_solve), "unit": UNIT,
                 "h2d_bytes_per_step": C.sizeof(cfg) / max(prog.iteration, 1),
                 "d2h_bytes_per_step": 8.0 * len(checks) / max(prog.iteration, 1),
