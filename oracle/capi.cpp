@@ -112,7 +112,29 @@ void oracle_destroy(void* h) { delete (Solver*)h; }
 
 void oracle_set_batch_river(void* h, int on) { ((Solver*)h)->batch_river = on != 0; }
 
-uint64_t oracle_storage_len(void* h) { return ((Solver*)h)->store.regrets.size(); }
+uint64_t oracle_storage_len(void* h) { return ((Solver*)h)->tree.storage_len; }
+int oracle_is_compressed(void* h) { return ((Solver*)h)->store.compressed ? 1 : 0; }
+uint64_t oracle_num_slots(void* h) { return ((Solver*)h)->tree.num_player_nodes; }
+// Compressed storage (storage.rs:92-97): i16 regrets, u16 sums, per-slot scales.
+int oracle_get_storage_compressed(void* h, int16_t* rq, uint16_t* sq, float* rscale, float* sscale) {
+  const Solver* s = (const Solver*)h;
+  if (!s->store.compressed) return 1;
+  std::memcpy(rq, s->store.rq.data(), s->store.rq.size() * 2);
+  std::memcpy(sq, s->store.sq.data(), s->store.sq.size() * 2);
+  std::memcpy(rscale, s->store.rscale.data(), s->store.rscale.size() * 4);
+  std::memcpy(sscale, s->store.sscale.data(), s->store.sscale.size() * 4);
+  return 0;
+}
+int oracle_set_storage_compressed(void* h, const int16_t* rq, const uint16_t* sq, const float* rscale,
+                                  const float* sscale) {
+  Solver* s = (Solver*)h;
+  if (!s->store.compressed) return 1;
+  std::memcpy(s->store.rq.data(), rq, s->store.rq.size() * 2);
+  std::memcpy(s->store.sq.data(), sq, s->store.sq.size() * 2);
+  std::memcpy(s->store.rscale.data(), rscale, s->store.rscale.size() * 4);
+  std::memcpy(s->store.sscale.data(), sscale, s->store.sscale.size() * 4);
+  return 0;
+}
 
 void oracle_get_storage(void* h, float* regrets, float* sums) {
   Solver* s = (Solver*)h;

@@ -653,14 +653,21 @@ static void normalize_in_place(float* s, size_t na, size_t n) {
 }
 
 // cfr.rs:196-207.
-static void positive_sums(const float* r, size_t na, size_t n, float* sums) {
-  for (size_t h = 0; h < n; h++) sums[h] = fmax0(r[h]);
+// Regrets as f32: stored f32, or undecoded i16 (regret matching is
+// invariant under the node's positive scale; cfr.rs:155-160).
+static inline float as_f32(float x) { return x; }
+static inline float as_f32(int16_t x) { return (float)x; }
+
+template <class T>
+static void positive_sums(const T* r, size_t na, size_t n, float* sums) {
+  for (size_t h = 0; h < n; h++) sums[h] = fmax0(as_f32(r[h]));
   for (size_t a = 1; a < na; a++)
-    for (size_t h = 0; h < n; h++) sums[h] += fmax0(r[a * n + h]);
+    for (size_t h = 0; h < n; h++) sums[h] += fmax0(as_f32(r[a * n + h]));
 }
 
 // cfr.rs:161-192.
-static void regret_match_into(const float* r, size_t na, size_t n, float* out) {
+template <class T>
+static void regret_match_into(const T* r, size_t na, size_t n, float* out) {
   if (n == 0) return;
   Buf inv(n);
   positive_sums(r, na, n, inv.data());
@@ -670,12 +677,97 @@ static void regret_match_into(const float* r, size_t na, size_t n, float* out) {
     any_zero |= inv[h] == 0.0f;
   }
   for (size_t a = 0; a < na; a++)
-    for (size_t h = 0; h < n; h++) out[a * n + h] = fmax0(r[a * n + h]) * inv[h];
+    for (size_t h = 0; h < n; h++) out[a * n + h] = fmax0(as_f32(r[a * n + h])) * inv[h];
   if (any_zero) {
     float uniform = 1.0f / (float)na;
     for (size_t h = 0; h < n; h++)
       if (inv[h] == 0.0f)
         for (size_t a = 0; a < na; a++) out[a * n + h] = uniform;
+  }
+}
+
+// ---- Storage accessors (storage.rs:226-330) ----
+// max(|x|) over a block (storage.rs:113-128; a max is order-free).
+static float max_abs(const float* v, size_t len) {
+  float m = 0.0f;
+  for (size_t i = 0; i < len; i++) m = std::fmax(m, std::fabs(v[i]));
+  return m;
+}
+
+// load_current_strategy (storage.rs:244-255).
+static void load_current_strategy(const Storage& st, const Node& node, size_t n, float* out) {
+  const size_t na = node.num_children;
+  if (st.compressed) regret_match_into(st.rq.data() + node.offset, na, n, out);
+  else regret_match_into(st.regrets.data() + node.offset, na, n, out);
+}
+
+// load_strat (storage.rs:256-268).
+static void load_strat(const Storage& st, const Node& node, size_t n, float* out) {
+  const size_t len = node.num_children * n;
+  if (!st.compressed) {
+    std::memcpy(out, st.strat.data() + node.offset, len * sizeof(float));
+    return;
+  }
+  const float scale = st.sscale[node.slot] / 65535.0f;
+  const uint16_t* q = st.sq.data() + node.offset;
+  for (size_t i = 0; i < len; i++) out[i] = (float)q[i] * scale;
+}
+
+// update_regrets (storage.rs:272-303): f on the decoded regrets, then the
+// node's new scale max|r| and round half away from zero, saturating.
+template <class F>
+static void update_regrets(Storage& st, const Node& node, size_t n, F f) {
+  const size_t len = node.num_children * n;
+  if (!st.compressed) {
+    f(st.regrets.data() + node.offset);
+    return;
+  }
+  Buf buf(len);
+  float& scale_slot = st.rscale[node.slot];
+  int16_t* q = st.rq.data() + node.offset;
+  const float scale = scale_slot / 32767.0f;
+  for (size_t i = 0; i < len; i++) buf[i] = (float)q[i] * scale;
+  f(buf.data());
+  const float mx = max_abs(buf.data(), len);
+  scale_slot = mx;
+  if (mx > 0.0f) {
+    const float inv = 32767.0f / mx;
+    for (size_t i = 0; i < len; i++) {
+      const float y = buf[i] * inv;
+      const float t = y + std::copysign(0.5f, y);
+      // Rust's `as i16`: truncation toward zero, saturating, NaN to 0.
+      q[i] = t != t ? (int16_t)0 : t >= 32767.0f ? (int16_t)32767 : t <= -32768.0f ? (int16_t)-32768 : (int16_t)t;
+    }
+  } else {
+    std::fill(q, q + len, (int16_t)0);
+  }
+}
+
+// update_strat (storage.rs:306-330): values kept non-negative, u16 with the
+// node's max, rounded half up.
+template <class F>
+static void update_strat(Storage& st, const Node& node, size_t n, F f) {
+  const size_t len = node.num_children * n;
+  if (!st.compressed) {
+    f(st.strat.data() + node.offset);
+    return;
+  }
+  Buf buf(len);
+  float& scale_slot = st.sscale[node.slot];
+  uint16_t* q = st.sq.data() + node.offset;
+  const float scale = scale_slot / 65535.0f;
+  for (size_t i = 0; i < len; i++) buf[i] = (float)q[i] * scale;
+  f(buf.data());
+  const float mx = max_abs(buf.data(), len);
+  scale_slot = mx;
+  if (mx > 0.0f) {
+    const float inv = 65535.0f / mx;
+    for (size_t i = 0; i < len; i++) {
+      const float t = std::fmax(buf[i], 0.0f) * inv + 0.5f;
+      q[i] = t != t ? (uint16_t)0 : t >= 65535.0f ? (uint16_t)65535 : (uint16_t)t;
+    }
+  } else {
+    std::fill(q, q + len, (uint16_t)0);
   }
 }
 
@@ -953,11 +1045,10 @@ void showdown_batch(const HandSet& hs, const StrengthTable& table, int p, const 
 static void traverse(const Ctx& ctx, size_t id, int p, const float* opp_reach, size_t nq, const Mode& mode, float* out,
                      size_t n);
 
-// own_node_update (cfr.rs:315-382) for F32 storage.
+// own_node_update (cfr.rs:315-382).
 static void own_node_update(const Ctx& ctx, const Node& node, size_t n, const float* cfv, const Mode& mode,
                             float* out) {
   size_t na = node.num_children;
-  size_t off = node.offset;
   if (mode.kind == MODE_BR) {
     for (size_t h = 0; h < n; h++) out[h] = cfv[h];
     for (size_t a = 1; a < na; a++)
@@ -966,13 +1057,14 @@ static void own_node_update(const Ctx& ctx, const Node& node, size_t n, const fl
         out[h] = v > out[h] ? v : out[h];
       }
   } else if (mode.kind == MODE_AVG) {
-    Buf s(ctx.store->strat.data() + off, na * n);
+    Buf s(na * n);
+    load_strat(*ctx.store, node, n, s.data());
     normalize_in_place(s.data(), na, n);
     for (size_t h = 0; h < n; h++) out[h] = 0.0f;
     for (size_t a = 0; a < na; a++)
       for (size_t h = 0; h < n; h++) out[h] += s[a * n + h] * cfv[a * n + h];
   } else {
-    float* r = ctx.store->regrets.data() + off;
+    update_regrets(*ctx.store, node, n, [&](float* r) {
     const Discount& d = mode.d;
     Buf inv(n);
     positive_sums(r, na, n, inv.data());
@@ -1000,6 +1092,7 @@ static void own_node_update(const Ctx& ctx, const Node& node, size_t n, const fl
         float disc = x > 0.0f ? d.pos : d.neg;
         r[a * n + h] = x * disc + cfv[a * n + h] - out[h];
       }
+    });
   }
 }
 
@@ -1019,21 +1112,21 @@ static void opponent_node(const Ctx& ctx, const Node& node, int p, const float* 
   size_t na = node.num_children;
   Buf s(na * nq);
   if (nq > 0) {
-    size_t off = node.offset;
     if (mode.kind == MODE_CFR) {
-      regret_match_into(ctx.store->regrets.data() + off, na, nq, s.data());
-      float* ss = ctx.store->strat.data() + off;
+      load_current_strategy(*ctx.store, node, nq, s.data());
       const Discount& d = mode.d;
-      for (size_t a = 0; a < na; a++)
-        for (size_t h = 0; h < nq; h++) {
-          float& x = ss[a * nq + h];
-          if (d.reach_weighted)
-            x = x * d.strat + s[a * nq + h] * opp_reach[h];
-          else
-            x = x * d.strat + s[a * nq + h];
-        }
+      update_strat(*ctx.store, node, nq, [&](float* ss) {
+        for (size_t a = 0; a < na; a++)
+          for (size_t h = 0; h < nq; h++) {
+            float& x = ss[a * nq + h];
+            if (d.reach_weighted)
+              x = x * d.strat + s[a * nq + h] * opp_reach[h];
+            else
+              x = x * d.strat + s[a * nq + h];
+          }
+      });
     } else {
-      std::memcpy(s.data(), ctx.store->strat.data() + off, na * nq * sizeof(float));
+      load_strat(*ctx.store, node, nq, s.data());
       normalize_in_place(s.data(), na, nq);
     }
     for (size_t a = 0; a < na; a++)
@@ -1164,22 +1257,22 @@ static void river_run(const Ctx& ctx, size_t root, int p, const float* opp_reach
       continue;
     }
     set_len_unzeroed(strat, na * nq);
-    size_t off = node.offset;
     if (mode.kind == MODE_CFR) {
-      regret_match_into(ctx.store->regrets.data() + off, na, nq, strat.data());
+      load_current_strategy(*ctx.store, node, nq, strat.data());
       const float* r = reach.data() + (size_t)it.reach * nq;
       float g = mode.d.strat;
-      float* ss = ctx.store->strat.data() + off;
-      for (size_t a = 0; a < na; a++)
-        for (size_t h = 0; h < nq; h++) {
-          float& x = ss[a * nq + h];
-          if (mode.d.reach_weighted)
-            x = x * g + strat[a * nq + h] * r[h];
-          else
-            x = x * g + strat[a * nq + h];
-        }
+      update_strat(*ctx.store, node, nq, [&](float* ss) {
+        for (size_t a = 0; a < na; a++)
+          for (size_t h = 0; h < nq; h++) {
+            float& x = ss[a * nq + h];
+            if (mode.d.reach_weighted)
+              x = x * g + strat[a * nq + h] * r[h];
+            else
+              x = x * g + strat[a * nq + h];
+          }
+      });
     } else {
-      std::memcpy(strat.data(), ctx.store->strat.data() + off, na * nq * sizeof(float));
+      load_strat(*ctx.store, node, nq, strat.data());
       normalize_in_place(strat.data(), na, nq);
     }
     size_t parent = (size_t)it.reach * nq;
@@ -1444,19 +1537,20 @@ std::unique_ptr<Solver> Solver::create(const SolveConfig& cfg, int& err, std::st
     msg = buf;
     return nullptr;
   }
-  if (st.compressed) {
-    // The oracle restates F32 storage only; 16-bit storage is not part of
-    // the restated path.
-    err = 8;
-    msg = "compressed storage is not restated by the oracle";
-    return nullptr;
-  }
   Builder b(tp);
   b.build(s->config.root);
   s->tree = std::move(b.tree);
   s->stats = st;
-  s->store.regrets.assign(s->tree.storage_len, 0.0f);
-  s->store.strat.assign(s->tree.storage_len, 0.0f);
+  s->store.compressed = st.compressed;
+  if (st.compressed) {
+    s->store.rq.assign(s->tree.storage_len, 0);
+    s->store.sq.assign(s->tree.storage_len, 0);
+    s->store.rscale.assign(s->tree.num_player_nodes, 0.0f);
+    s->store.sscale.assign(s->tree.num_player_nodes, 0.0f);
+  } else {
+    s->store.regrets.assign(s->tree.storage_len, 0.0f);
+    s->store.strat.assign(s->tree.storage_len, 0.0f);
+  }
   s->tables.resize(s->tree.boards.size());
   for (size_t i = 0; i < s->tree.boards.size(); i++) s->tables[i].build(s->hands, s->tree.boards[i]);
   s->iterations = 0;
@@ -1559,7 +1653,7 @@ std::vector<float> Solver::average_strategy(size_t id, size_t n) const {
   const Node& node = tree.nodes[id];
   std::vector<float> s(node.num_children * n, 0.0f);
   if (n > 0) {
-    std::memcpy(s.data(), store.strat.data() + node.offset, s.size() * sizeof(float));
+    load_strat(store, node, n, s.data());
     normalize_in_place(s.data(), node.num_children, n);
   }
   return s;

@@ -172,9 +172,15 @@ struct Isomorphism {
                     std::vector<IsoRef>& refs) const;
 };
 
-// Storage::F32 (storage.rs:87-98).
+// Storage (storage.rs:87-98): F32, or Compressed (16-bit values with one
+// f32 scale per player node slot: regrets i16 scaled by max|r| / 32767,
+// strategy sums u16 scaled by max / 65535).
 struct Storage {
-  std::vector<float> regrets, strat;
+  bool compressed = false;
+  std::vector<float> regrets, strat;  // F32
+  std::vector<int16_t> rq;            // Compressed
+  std::vector<uint16_t> sq;
+  std::vector<float> rscale, sscale;  // per player node slot
 };
 
 enum ModeKind { MODE_CFR = 0, MODE_BR = 1, MODE_AVG = 2 };

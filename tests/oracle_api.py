@@ -41,6 +41,11 @@ def lib():
         L.oracle_storage_len.restype = C.c_uint64
         L.oracle_storage_len.argtypes = [P]
         L.oracle_get_storage.argtypes = [P, P, P]
+        L.oracle_is_compressed.argtypes = [P]
+        L.oracle_num_slots.restype = C.c_uint64
+        L.oracle_num_slots.argtypes = [P]
+        L.oracle_get_storage_compressed.argtypes = [P, P, P, P, P]
+        L.oracle_set_storage_compressed.argtypes = [P, P, P, P, P]
         L.oracle_set_storage.argtypes = [P, P, P]
         L.oracle_set_iterations.argtypes = [P, C.c_uint32]
         L.oracle_iterations.restype = C.c_uint32
@@ -171,6 +176,29 @@ class OracleSolver:
         s = np.ascontiguousarray(s, np.float32)
         assert len(r) == lib().oracle_storage_len(self.h)
         lib().oracle_set_storage(self.h, ptr(r), ptr(s))
+
+    @property
+    def compressed(self) -> bool:
+        return bool(lib().oracle_is_compressed(self.h))
+
+    def compressed_storage(self):
+        """(i16 regrets, u16 sums, regret scales, sum scales) of a compressed
+        solver (storage.rs:92-97)."""
+        n = lib().oracle_storage_len(self.h)
+        k = lib().oracle_num_slots(self.h)
+        rq = np.zeros(n, np.int16)
+        sq = np.zeros(n, np.uint16)
+        rs = np.zeros(k, np.float32)
+        ss = np.zeros(k, np.float32)
+        assert lib().oracle_get_storage_compressed(self.h, ptr(rq), ptr(sq), ptr(rs), ptr(ss)) == 0
+        return rq, sq, rs, ss
+
+    def set_compressed_storage(self, rq, sq, rs, ss):
+        rq = np.ascontiguousarray(rq, np.int16)
+        sq = np.ascontiguousarray(sq, np.uint16)
+        rs = np.ascontiguousarray(rs, np.float32)
+        ss = np.ascontiguousarray(ss, np.float32)
+        assert lib().oracle_set_storage_compressed(self.h, ptr(rq), ptr(sq), ptr(rs), ptr(ss)) == 0
 
     def set_iterations(self, t):
         lib().oracle_set_iterations(self.h, t)
