@@ -304,10 +304,25 @@ int dcfr_ranges_after(dcfr_solver* s, const dcfr_step* path, size_t n, float out
 /* Storage in the reference layout (storage.rs:87-98; one action-major
  * block per decision node at Node::offset, tree.rs:200-204): len f32
  * regrets and len f32 strategy sums. Used to resume a solve elsewhere
- * (lib.rs:532-540) and by the parity tests. */
+ * (lib.rs:532-540) and by the parity tests. A solver with compressed
+ * storage downloads its values decoded (load_regrets / load_strat,
+ * storage.rs:226-268) and uploads only through the compressed call. */
 int dcfr_storage_len(const dcfr_solver* s, uint64_t* len);
 int dcfr_download_storage(dcfr_solver* s, float* regrets, float* sums, uint64_t len);
 int dcfr_upload_storage(dcfr_solver* s, const float* regrets, const float* sums, uint64_t len);
+/* Compressed storage (Storage::Compressed, storage.rs:92-97; chosen by
+ * DCFR_STORAGE_COMPRESSED, or by DCFR_STORAGE_AUTO when the f32 tree would
+ * exceed 1 GB, as StorageMode::Auto): len i16 regrets and len u16 strategy
+ * sums in the reference layout, and per decision node slot (Node::slot,
+ * tree.rs:463) one f32 regret scale and one f32 sum scale; the stored
+ * values decode as regret * scale / 32767 and sum * scale / 65535. The
+ * HostStorage::Compressed transfer of the reference's GPU engine
+ * (gpu/engine.rs:292-425). */
+int dcfr_storage_slots(const dcfr_solver* s, uint64_t* slots);
+int dcfr_download_storage_compressed(dcfr_solver* s, int16_t* regrets, uint16_t* sums, float* regret_scale,
+                                     float* sum_scale, uint64_t len, uint64_t slots);
+int dcfr_upload_storage_compressed(dcfr_solver* s, const int16_t* regrets, const uint16_t* sums,
+                                   const float* regret_scale, const float* sum_scale, uint64_t len, uint64_t slots);
 /* Sets the iteration counter (after uploading storage from another run). */
 int dcfr_set_iterations(dcfr_solver* s, uint32_t t);
 

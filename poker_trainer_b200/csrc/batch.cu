@@ -400,6 +400,11 @@ Status Batch::Impl::init(const dcfr_config* cfgs, int count) {
       s.msg = "spot " + std::to_string(i) + ": " + msg;
       return s;
     }
+    if (games[i].compressed) {
+      s.code = DCFR_ERR_UNSUPPORTED;
+      s.msg = "spot " + std::to_string(i) + ": the batched solve runs f32 storage";
+      return s;
+    }
   }
   // Host plans and the layout of every device array.
   std::vector<DownTask> hdown;

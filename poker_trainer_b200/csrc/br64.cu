@@ -47,6 +47,15 @@ __device__ __forceinline__ void st4d(double* p, const double (&x)[V64]) {
 }
 
 // Opponent split by the average strategy, or chance split.
+// One node's strategy sums for 4 hands as f32: stored f32, or the 16-bit
+// sums decoded with the node's scale (load_strat, storage.rs:256-268).
+__device__ __forceinline__ float4 sums4(const Row64Args& A, uint64_t store, uint32_t slot, size_t off) {
+  if (A.sq == nullptr) return *reinterpret_cast<const float4*>(A.sums + store + off);
+  const float sc = A.sscale[slot] / 65535.0f;
+  const ushort4 q = *reinterpret_cast<const ushort4*>(A.sq + store + off);
+  return make_float4((float)q.x * sc, (float)q.y * sc, (float)q.z * sc, (float)q.w * sc);
+}
+
 __device__ void down64_item(const Row64Args& A, const DownTask& T, int h0, int lane) {
   if (A.alive[T.in_slot] == 0) return;
   const int o = A.p ^ 1;
@@ -58,10 +67,9 @@ __device__ void down64_item(const Row64Args& A, const DownTask& T, int h0, int l
   if ((T.kind & KIND_MASK) == D_OPP_SPLIT) {
     const int na = (int)T.nchild;
     double tot[V64] = {0.0, 0.0, 0.0, 0.0};
-    const float* base = A.sums + T.store + h0;
     for (int a = 0; a < na; a++)
       if (valid) {
-        const float4 s = *reinterpret_cast<const float4*>(base + (size_t)a * hp);
+        const float4 s = sums4(A, T.store, T.cards, (size_t)a * hp + h0);
         tot[0] += (double)s.x;
         tot[1] += (double)s.y;
         tot[2] += (double)s.z;
@@ -70,7 +78,7 @@ __device__ void down64_item(const Row64Args& A, const DownTask& T, int h0, int l
     for (int a = 0; a < na; a++) {
       double c[V64] = {0.0, 0.0, 0.0, 0.0};
       if (valid) {
-        const float4 s = *reinterpret_cast<const float4*>(base + (size_t)a * hp);
+        const float4 s = sums4(A, T.store, T.cards, (size_t)a * hp + h0);
         const double sv[V64] = {(double)s.x, (double)s.y, (double)s.z, (double)s.w};
 #pragma unroll
         for (int j = 0; j < V64; j++) {
@@ -127,17 +135,16 @@ __device__ void up64_item(const Row64Args& A, const UpTask& T, int h0) {
         for (int j = 0; j < V64; j++) out[j] = v[j] > out[j] ? v[j] : out[j];
       }
     } else {
-      const float* base = A.sums + T.store + h0;
       double tot[V64] = {0.0, 0.0, 0.0, 0.0};
       for (int a = 0; a < na; a++) {
-        const float4 s = *reinterpret_cast<const float4*>(base + (size_t)a * hp);
+        const float4 s = sums4(A, T.store, T.cards, (size_t)a * hp + h0);
         tot[0] += (double)s.x;
         tot[1] += (double)s.y;
         tot[2] += (double)s.z;
         tot[3] += (double)s.w;
       }
       for (int a = 0; a < na; a++) {
-        const float4 s = *reinterpret_cast<const float4*>(base + (size_t)a * hp);
+        const float4 s = sums4(A, T.store, T.cards, (size_t)a * hp + h0);
         const double sv[V64] = {(double)s.x, (double)s.y, (double)s.z, (double)s.w};
         double v[V64];
         ld4d(A.vals + (size_t)(T.child + a) * stride + h0, v);

@@ -359,6 +359,33 @@ int dcfr_upload_storage(dcfr_solver* s, const float* regrets, const float* sums,
   GUARD_END
 }
 
+int dcfr_storage_slots(const dcfr_solver* s, uint64_t* slots) {
+  NEED(s);
+  if (!slots) return fail(DCFR_ERR_INVALID_ARG, "NULL argument");
+  *slots = s->e->slots();
+  return DCFR_OK;
+}
+
+int dcfr_download_storage_compressed(dcfr_solver* s, int16_t* regrets, uint16_t* sums, float* regret_scale,
+                                     float* sum_scale, uint64_t len, uint64_t slots) {
+  NEED(s);
+  if (len != s->e->g.storage_len || slots != s->e->slots())
+    return fail(DCFR_ERR_INVALID_ARG, "storage length or slot count mismatch");
+  GUARD_BEGIN
+  return done(s->e->download_compressed(regrets, sums, regret_scale, sum_scale));
+  GUARD_END
+}
+
+int dcfr_upload_storage_compressed(dcfr_solver* s, const int16_t* regrets, const uint16_t* sums,
+                                   const float* regret_scale, const float* sum_scale, uint64_t len, uint64_t slots) {
+  NEED(s);
+  if (len != s->e->g.storage_len || slots != s->e->slots() || !regrets || !sums || !regret_scale || !sum_scale)
+    return fail(DCFR_ERR_INVALID_ARG, "storage length or slot count mismatch");
+  GUARD_BEGIN
+  return done(s->e->upload_compressed(regrets, sums, regret_scale, sum_scale));
+  GUARD_END
+}
+
 int dcfr_set_iterations(dcfr_solver* s, uint32_t t) {
   NEED(s);
   return done(s->e->set_iterations(t));

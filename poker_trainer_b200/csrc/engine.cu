@@ -132,6 +132,7 @@ Status Engine::create_depth_limited(const dcfr_config& cfg, dcfr_mlp* net, int l
   e->fast_ = true;
   s.code = build_game(cfg, e->g, s.msg, true, leaf_street);
   if (!s.ok()) return s;
+  if (e->g.compressed) return Status{DCFR_ERR_UNSUPPORTED, "depth-limited solves run f32 storage"};
   e->net_ = net;
   if (!(s = e->init()).ok()) return s;
   if (!(s = e->init_leaves()).ok()) return s;
@@ -146,6 +147,10 @@ Engine::~Engine() {
   full_[1].reset();
   dfree(regrets_);
   dfree(sums_);
+  dfree(rq_);
+  dfree(sq_);
+  dfree(rscale_);
+  dfree(sscale_);
   dfree(reach_);
   dfree(vals_);
   dfree(alive_);
@@ -245,10 +250,25 @@ Status Engine::init() {
     gpu_len_ += (uint64_t)g.nodes[v].nchild * (uint64_t)hp_[g.nodes[v].player];
   }
   Status s;
-  if (!(s = dalloc(regrets_, gpu_len_, "storage")).ok()) return s;
-  if (!(s = dalloc(sums_, gpu_len_, "storage")).ok()) return s;
-  CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
-  CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
+  compressed_ = g.compressed;
+  if (compressed_) {
+    // Storage::Compressed (storage.rs:92-97): 16-bit values, a scale of
+    // each kind per decision node (its ordinal, the reference's slot).
+    const size_t slots = std::max<size_t>(g.player_nodes, 1);
+    if (!(s = dalloc(rq_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(sq_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(rscale_, slots, "storage scales")).ok()) return s;
+    if (!(s = dalloc(sscale_, slots, "storage scales")).ok()) return s;
+    CK(cudaMemsetAsync(rq_, 0, gpu_len_ * 2, stream_));
+    CK(cudaMemsetAsync(sq_, 0, gpu_len_ * 2, stream_));
+    CK(cudaMemsetAsync(rscale_, 0, slots * 4, stream_));
+    CK(cudaMemsetAsync(sscale_, 0, slots * 4, stream_));
+  } else {
+    if (!(s = dalloc(regrets_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(sums_, gpu_len_, "storage")).ok()) return s;
+    CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
+    CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
+  }
 
   tstride_ = std::max(g.n[0], g.n[1]);
   pstride_ = (2 * tstride_ + TERM_CHUNK - 1) / TERM_CHUNK * TERM_CHUNK;
@@ -536,9 +556,11 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
         s.msg = "a decision node has more than 16 actions";
         return s;
       }
-      if (!own) fdown[tree].push_back({tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f}});
+      // `cards` of a decision node's tasks: its scale slot (compressed storage).
+      if (!own)
+        fdown[tree].push_back({tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], nd.index, 0.0f}});
       fup[tree].push_back({tdepth, UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
-                                          first_slot, gpu_off_[v], 0, 0, 0, 0}});
+                                          first_slot, gpu_off_[v], nd.index, 0, 0, 0}});
       fmaxa = std::max<int>(fmaxa, (int)nd.nchild);
     } else if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
       // Chance nodes, by layer (decision nodes all belong to segments).
@@ -575,9 +597,10 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
           sdown[layer].resize(sd + 1);
           sup[layer].resize(sd + 1);
         }
-        if (!own) sdown[layer][sd].push_back(DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], 0, 0.0f});
+        if (!own)
+          sdown[layer][sd].push_back(DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], nd.index, 0.0f});
         sup[layer][sd].push_back(UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
-                                        first_slot, gpu_off_[v], 0, 0, 0, 0});
+                                        first_slot, gpu_off_[v], nd.index, 0, 0, 0});
       } else {
         DownTask t{D_CHANCE_SPLIT, sv, first_slot, nd.nchild, 0, cc_off_[nd.index], nd.factor};
         down[depth].push_back(t);
@@ -896,6 +919,11 @@ Status Engine::upload_plan(Plan& plan) {
 void Engine::row_args(int p, RowArgs& A) const {
   A.regrets = regrets_;
   A.sums = sums_;
+  A.rq = rq_;
+  A.sq = sq_;
+  A.rscale = rscale_;
+  A.sscale = sscale_;
+  A.compressed = compressed_ ? 1 : 0;
   A.reach = reach_;
   A.vals = vals_;
   A.alive = alive_;
@@ -1134,6 +1162,7 @@ Status Engine::write_node(const std::vector<dcfr_step>& path, const float* regre
   if (!s.ok()) return s;
   const GNode& nd = g.nodes[node];
   if (nd.kind != N_PLAYER) return bad_path("not a decision node");
+  if (compressed_) return Status{DCFR_ERR_UNSUPPORTED, "write_node takes f32 storage"};
   const int q = nd.player, n = g.n[q];
   for (int a = 0; a < nd.nchild; a++) {
     if (sums)
@@ -1355,6 +1384,8 @@ Status Engine::fp64_root_values(int mode, double out[2]) {
                        stream_));
     Row64Args A;
     A.sums = sums_;
+    A.sq = compressed_ ? sq_ : nullptr;
+    A.sscale = sscale_;
     A.reach = reach64_;
     A.vals = vals64_;
     A.alive = alive_;
@@ -1511,9 +1542,28 @@ Status Engine::solve(const dcfr_solve_options& opts, const volatile int32_t* can
 
 Status Engine::download(float* regrets, float* sums) {
   std::vector<float> r(gpu_len_), sm(gpu_len_);
-  CK(cudaMemcpyAsync(r.data(), regrets_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
-  CK(cudaMemcpyAsync(sm.data(), sums_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamSynchronize(stream_));
+  if (compressed_) {
+    // Decoded as load_regrets / load_strat do (storage.rs:226-268).
+    std::vector<int16_t> rq(gpu_len_);
+    std::vector<uint16_t> sq(gpu_len_);
+    std::vector<float> rs, ss;
+    Status s = download_compressed_raw(rq, sq, rs, ss);
+    if (!s.ok()) return s;
+    for (uint32_t v = 0; v < g.nodes.size(); v++) {
+      const GNode& nd = g.nodes[v];
+      if (nd.kind != N_PLAYER) continue;
+      const size_t len = (size_t)nd.nchild * hp_[nd.player];
+      const float rsc = rs[nd.index] / 32767.0f, ssc = ss[nd.index] / 65535.0f;
+      for (size_t i = 0; i < len; i++) {
+        r[gpu_off_[v] + i] = (float)rq[gpu_off_[v] + i] * rsc;
+        sm[gpu_off_[v] + i] = (float)sq[gpu_off_[v] + i] * ssc;
+      }
+    }
+  } else {
+    CK(cudaMemcpyAsync(r.data(), regrets_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(sm.data(), sums_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+  }
   for (uint32_t v = 0; v < g.nodes.size(); v++) {
     const GNode& nd = g.nodes[v];
     if (nd.kind != N_PLAYER) continue;
@@ -1527,7 +1577,69 @@ Status Engine::download(float* regrets, float* sums) {
   return Status();
 }
 
+Status Engine::download_compressed_raw(std::vector<int16_t>& rq, std::vector<uint16_t>& sq, std::vector<float>& rs,
+                                       std::vector<float>& ss) {
+  const size_t slots = std::max<size_t>(g.player_nodes, 1);
+  rq.resize(gpu_len_);
+  sq.resize(gpu_len_);
+  rs.resize(slots);
+  ss.resize(slots);
+  CK(cudaMemcpyAsync(rq.data(), rq_, gpu_len_ * 2, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(sq.data(), sq_, gpu_len_ * 2, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(rs.data(), rscale_, slots * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(ss.data(), sscale_, slots * 4, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+Status Engine::download_compressed(int16_t* regrets, uint16_t* sums, float* rscale, float* sscale) {
+  if (!compressed_) return Status{DCFR_ERR_UNSUPPORTED, "the solver's storage is f32"};
+  std::vector<int16_t> rq;
+  std::vector<uint16_t> sq;
+  std::vector<float> rs, ss;
+  Status s = download_compressed_raw(rq, sq, rs, ss);
+  if (!s.ok()) return s;
+  for (uint32_t v = 0; v < g.nodes.size(); v++) {
+    const GNode& nd = g.nodes[v];
+    if (nd.kind != N_PLAYER) continue;
+    const int q = nd.player, n = g.n[q];
+    for (int a = 0; a < nd.nchild; a++) {
+      if (regrets)
+        std::memcpy(regrets + nd.ref_offset + (size_t)a * n, rq.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 2);
+      if (sums) std::memcpy(sums + nd.ref_offset + (size_t)a * n, sq.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 2);
+    }
+  }
+  if (rscale) std::memcpy(rscale, rs.data(), (size_t)g.player_nodes * 4);
+  if (sscale) std::memcpy(sscale, ss.data(), (size_t)g.player_nodes * 4);
+  return Status();
+}
+
+Status Engine::upload_compressed(const int16_t* regrets, const uint16_t* sums, const float* rscale,
+                                 const float* sscale) {
+  if (!compressed_) return Status{DCFR_ERR_UNSUPPORTED, "the solver's storage is f32"};
+  std::vector<int16_t> rq(gpu_len_, 0);
+  std::vector<uint16_t> sq(gpu_len_, 0);
+  for (uint32_t v = 0; v < g.nodes.size(); v++) {
+    const GNode& nd = g.nodes[v];
+    if (nd.kind != N_PLAYER) continue;
+    const int q = nd.player, n = g.n[q];
+    for (int a = 0; a < nd.nchild; a++) {
+      std::memcpy(rq.data() + gpu_off_[v] + (size_t)a * hp_[q], regrets + nd.ref_offset + (size_t)a * n, n * 2);
+      std::memcpy(sq.data() + gpu_off_[v] + (size_t)a * hp_[q], sums + nd.ref_offset + (size_t)a * n, n * 2);
+    }
+  }
+  CK(cudaMemcpyAsync(rq_, rq.data(), gpu_len_ * 2, cudaMemcpyHostToDevice, stream_));
+  CK(cudaMemcpyAsync(sq_, sq.data(), gpu_len_ * 2, cudaMemcpyHostToDevice, stream_));
+  if (g.player_nodes) {
+    CK(cudaMemcpyAsync(rscale_, rscale, (size_t)g.player_nodes * 4, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(sscale_, sscale, (size_t)g.player_nodes * 4, cudaMemcpyHostToDevice, stream_));
+  }
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
 Status Engine::upload(const float* regrets, const float* sums) {
+  if (compressed_) return Status{DCFR_ERR_UNSUPPORTED, "compressed storage: use dcfr_upload_storage_compressed"};
   std::vector<float> r(gpu_len_, 0.0f), sm(gpu_len_, 0.0f);
   for (uint32_t v = 0; v < g.nodes.size(); v++) {
     const GNode& nd = g.nodes[v];
@@ -1556,8 +1668,18 @@ Status Engine::avg_strategy(uint32_t node, std::vector<float>& s) {
   const GNode& nd = g.nodes[node];
   int q = nd.player, n = g.n[q];
   std::vector<float> blk((size_t)nd.nchild * hp_[q]);
-  CK(cudaMemcpyAsync(blk.data(), sums_ + gpu_off_[node], blk.size() * 4, cudaMemcpyDeviceToHost, stream_));
-  CK(cudaStreamSynchronize(stream_));
+  if (compressed_) {
+    std::vector<uint16_t> q16(blk.size());
+    float sc = 0.0f;
+    CK(cudaMemcpyAsync(q16.data(), sq_ + gpu_off_[node], q16.size() * 2, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(&sc, sscale_ + nd.index, 4, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const float dec = sc / 65535.0f;
+    for (size_t i = 0; i < blk.size(); i++) blk[i] = (float)q16[i] * dec;
+  } else {
+    CK(cudaMemcpyAsync(blk.data(), sums_ + gpu_off_[node], blk.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+  }
   s.assign((size_t)nd.nchild * n, 0.0f);
   for (int a = 0; a < nd.nchild; a++)
     std::memcpy(s.data() + (size_t)a * n, blk.data() + (size_t)a * hp_[q], n * 4);

@@ -175,6 +175,12 @@ class Engine {
                dcfr_progress& out);
   Status download(float* regrets, float* sums);
   Status upload(const float* regrets, const float* sums);
+  // 16-bit compressed storage in the reference layout (storage.rs:92-97):
+  // len values of each kind, one scale of each kind per decision node slot.
+  bool compressed() const { return compressed_; }
+  uint64_t slots() const { return g.player_nodes; }
+  Status download_compressed(int16_t* regrets, uint16_t* sums, float* rscale, float* sscale);
+  Status upload_compressed(const int16_t* regrets, const uint16_t* sums, const float* rscale, const float* sscale);
   Status set_iterations(uint32_t t);
   Status query(const std::vector<dcfr_step>& path, dcfr_node_info& info, std::vector<Act>& actions,
                std::vector<uint16_t>& combos, std::vector<float>& strategy, std::vector<float>& ev,
@@ -199,6 +205,13 @@ class Engine {
   // Device buffers.
   float* regrets_ = nullptr;
   float* sums_ = nullptr;
+  bool compressed_ = false;
+  int16_t* rq_ = nullptr;   // compressed storage (GPU layout) and per-slot scales
+  uint16_t* sq_ = nullptr;
+  float* rscale_ = nullptr;
+  float* sscale_ = nullptr;
+  Status download_compressed_raw(std::vector<int16_t>& rq, std::vector<uint16_t>& sq, std::vector<float>& rs,
+                                 std::vector<float>& ss);
   float* reach_ = nullptr;
   float* vals_ = nullptr;
   uint32_t* alive_ = nullptr;

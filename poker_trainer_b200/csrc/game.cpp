@@ -602,10 +602,6 @@ int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tre
     msg = buf;
     return DCFR_ERR_TOO_LARGE;
   }
-  if (g.compressed) {
-    msg = "16-bit compressed storage is not built in this library; use DCFR_STORAGE_F32";
-    return DCFR_ERR_UNSUPPORTED;
-  }
   g.nodes.clear();
   g.chance.clear();
   g.boards.clear();

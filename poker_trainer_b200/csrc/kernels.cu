@@ -26,25 +26,26 @@ namespace dcfr {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
-template <int MODE, int MAXA>
+// COMP: 16-bit compressed storage (one block covers a node's row).
+template <int MODE, int MAXA, bool COMP>
 __global__ void __launch_bounds__(ROW_MAX_THREADS) down_kernel(RowArgs A, const DownTask* __restrict__ tasks,
                                                                int chunks) {
   const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
   const DownTask T = tasks[t];  // plan data: readable before the wait
   pdl_wait();
   const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
-  if (T.kind == D_OPP_SPLIT) down_item<MODE, MAXA, D_OPP_SPLIT>(A, T, h0, threadIdx.x & 31);
+  if (T.kind == D_OPP_SPLIT) down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, threadIdx.x & 31);
   else down_item<MODE, 1, D_CHANCE_SPLIT>(A, T, h0, threadIdx.x & 31);
   pdl_launch_dependents();
 }
 
-template <int MODE, int MAXA>
+template <int MODE, int MAXA, bool COMP>
 __global__ void __launch_bounds__(ROW_MAX_THREADS) up_kernel(RowArgs A, const UpTask* __restrict__ tasks, int chunks) {
   const int t = blockIdx.x / chunks, ch = blockIdx.x - t * chunks;
   const UpTask T = tasks[t];
   pdl_wait();
   const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
-  if (T.kind == U_OWN) up_item<MODE, MAXA, U_OWN>(A, T, h0);
+  if (T.kind == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0);
   else if (T.kind == U_OPP_SUM) up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
   else up_item<MODE, 1, U_CHANCE_SUM>(A, T, h0);
   pdl_launch_dependents();
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) up_kernel(RowArgs A, const Up
 // FusedTree). Every thread keeps the same 4 hands throughout, so a node's
 // rows are produced and consumed by the same threads; the barrier between
 // down levels publishes the children's liveness flags.
-template <int MODE, int MAXA>
+template <int MODE, int MAXA, bool COMP>
 __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_down_kernel(RowArgs A, const FusedTree* __restrict__ trees,
                                                                      const DownTask* __restrict__ tasks) {
   const FusedTree F = trees[blockIdx.x];
@@ -64,12 +65,12 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_down_kernel(RowArgs A, 
   for (uint32_t i = 0; i < F.down_count; i++) {
     const DownTask T = tasks[F.down_first + i];
     if (T.kind & LEVEL_BREAK) __syncthreads();
-    down_item<MODE, MAXA, D_OPP_SPLIT>(A, T, h0, lane);
+    down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, lane);
   }
   pdl_launch_dependents();
 }
 
-template <int MODE, int MAXA>
+template <int MODE, int MAXA, bool COMP>
 __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_up_kernel(RowArgs A, const FusedTree* __restrict__ trees,
                                                                    const UpTask* __restrict__ tasks) {
   const FusedTree F = trees[blockIdx.x];
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_up_kernel(RowArgs A, co
 #pragma unroll 1
   for (uint32_t i = 0; i < F.up_count; i++) {
     const UpTask T = tasks[F.up_first + i];
-    if ((T.kind & KIND_MASK) == U_OWN) up_item<MODE, MAXA, U_OWN>(A, T, h0);
+    if ((T.kind & KIND_MASK) == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0);
     else up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
   }
   pdl_launch_dependents();
@@ -284,16 +285,26 @@ static void launch_level(K kernel, const RowArgs& A, const Task* tasks, int ntas
 
 template <int MODE>
 static void launch_down_m(int maxa, const RowArgs& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s) {
-  if (maxa <= 4) return launch_level(down_kernel<MODE, 4>, A, tasks, ntasks, hp, s);
-  if (maxa <= 8) return launch_level(down_kernel<MODE, 8>, A, tasks, ntasks, hp, s);
-  launch_level(down_kernel<MODE, MAX_ACTIONS>, A, tasks, ntasks, hp, s);
+  if (A.compressed) {
+    if (maxa <= 4) return launch_level(down_kernel<MODE, 4, true>, A, tasks, ntasks, hp, s);
+    if (maxa <= 8) return launch_level(down_kernel<MODE, 8, true>, A, tasks, ntasks, hp, s);
+    return launch_level(down_kernel<MODE, MAX_ACTIONS, true>, A, tasks, ntasks, hp, s);
+  }
+  if (maxa <= 4) return launch_level(down_kernel<MODE, 4, false>, A, tasks, ntasks, hp, s);
+  if (maxa <= 8) return launch_level(down_kernel<MODE, 8, false>, A, tasks, ntasks, hp, s);
+  launch_level(down_kernel<MODE, MAX_ACTIONS, false>, A, tasks, ntasks, hp, s);
 }
 
 template <int MODE>
 static void launch_up_m(int maxa, const RowArgs& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s) {
-  if (maxa <= 4) return launch_level(up_kernel<MODE, 4>, A, tasks, ntasks, hp, s);
-  if (maxa <= 8) return launch_level(up_kernel<MODE, 8>, A, tasks, ntasks, hp, s);
-  launch_level(up_kernel<MODE, MAX_ACTIONS>, A, tasks, ntasks, hp, s);
+  if (A.compressed) {
+    if (maxa <= 4) return launch_level(up_kernel<MODE, 4, true>, A, tasks, ntasks, hp, s);
+    if (maxa <= 8) return launch_level(up_kernel<MODE, 8, true>, A, tasks, ntasks, hp, s);
+    return launch_level(up_kernel<MODE, MAX_ACTIONS, true>, A, tasks, ntasks, hp, s);
+  }
+  if (maxa <= 4) return launch_level(up_kernel<MODE, 4, false>, A, tasks, ntasks, hp, s);
+  if (maxa <= 8) return launch_level(up_kernel<MODE, 8, false>, A, tasks, ntasks, hp, s);
+  launch_level(up_kernel<MODE, MAX_ACTIONS, false>, A, tasks, ntasks, hp, s);
 }
 
 template <typename K, typename Task>
@@ -315,14 +326,24 @@ static void launch_fused(K kernel, const RowArgs& A, const FusedTree* trees, int
 template <int MODE>
 static void launch_fused_m(bool up, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees,
                            const DownTask* dt, const UpTask* ut, int hp, cudaStream_t s) {
-  if (up) {
-    if (maxa <= 4) return launch_fused(fused_up_kernel<MODE, 4>, A, trees, ntrees, ut, hp, s);
-    if (maxa <= 8) return launch_fused(fused_up_kernel<MODE, 8>, A, trees, ntrees, ut, hp, s);
-    return launch_fused(fused_up_kernel<MODE, MAX_ACTIONS>, A, trees, ntrees, ut, hp, s);
+  if (A.compressed) {
+    if (up) {
+      if (maxa <= 4) return launch_fused(fused_up_kernel<MODE, 4, true>, A, trees, ntrees, ut, hp, s);
+      if (maxa <= 8) return launch_fused(fused_up_kernel<MODE, 8, true>, A, trees, ntrees, ut, hp, s);
+      return launch_fused(fused_up_kernel<MODE, MAX_ACTIONS, true>, A, trees, ntrees, ut, hp, s);
+    }
+    if (maxa <= 4) return launch_fused(fused_down_kernel<MODE, 4, true>, A, trees, ntrees, dt, hp, s);
+    if (maxa <= 8) return launch_fused(fused_down_kernel<MODE, 8, true>, A, trees, ntrees, dt, hp, s);
+    return launch_fused(fused_down_kernel<MODE, MAX_ACTIONS, true>, A, trees, ntrees, dt, hp, s);
   }
-  if (maxa <= 4) return launch_fused(fused_down_kernel<MODE, 4>, A, trees, ntrees, dt, hp, s);
-  if (maxa <= 8) return launch_fused(fused_down_kernel<MODE, 8>, A, trees, ntrees, dt, hp, s);
-  launch_fused(fused_down_kernel<MODE, MAX_ACTIONS>, A, trees, ntrees, dt, hp, s);
+  if (up) {
+    if (maxa <= 4) return launch_fused(fused_up_kernel<MODE, 4, false>, A, trees, ntrees, ut, hp, s);
+    if (maxa <= 8) return launch_fused(fused_up_kernel<MODE, 8, false>, A, trees, ntrees, ut, hp, s);
+    return launch_fused(fused_up_kernel<MODE, MAX_ACTIONS, false>, A, trees, ntrees, ut, hp, s);
+  }
+  if (maxa <= 4) return launch_fused(fused_down_kernel<MODE, 4, false>, A, trees, ntrees, dt, hp, s);
+  if (maxa <= 8) return launch_fused(fused_down_kernel<MODE, 8, false>, A, trees, ntrees, dt, hp, s);
+  launch_fused(fused_down_kernel<MODE, MAX_ACTIONS, false>, A, trees, ntrees, dt, hp, s);
 }
 
 void launch_fused_down(int mode, int maxa, const RowArgs& A, const FusedTree* trees, int ntrees,

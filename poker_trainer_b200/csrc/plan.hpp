@@ -36,7 +36,8 @@ struct DownTask {
   uint32_t out_slot;  // slot of the first child (children's slots are consecutive)
   uint32_t nchild;
   uint64_t store;     // opponent split: float offset of the node's block
-  uint32_t cards;     // chance split: offset of the children's cards in chance_cards
+  uint32_t cards;     // chance split: offset of the children's cards in chance_cards;
+                      // opponent split: the node's scale slot (compressed storage)
   float factor;       // chance split: reach multiplier
 };
 
@@ -48,7 +49,8 @@ struct UpTask {
   uint32_t nchild;
   uint32_t child_slot;  // first child's slot (opponent / chance nodes)
   uint64_t store;       // traverser node: float offset of its block
-  uint32_t cards;       // chance: offset of the children's cards
+  uint32_t cards;       // chance: offset of the children's cards; decision node:
+                        // its scale slot (compressed storage)
   uint32_t iso_first;   // chance: first isomorphic reference
   uint32_t iso_count;
   uint32_t pad;
@@ -187,6 +189,13 @@ using FastArgs64 = FastArgsT<double>;
 struct RowArgs {
   float* regrets;
   float* sums;
+  // 16-bit compressed storage (set instead of regrets / sums): i16 regrets,
+  // u16 sums, one f32 scale of each per decision node (its ordinal).
+  int16_t* rq;
+  uint16_t* sq;
+  float* rscale;
+  float* sscale;
+  int compressed;
   float* reach;
   float* vals;
   uint32_t* alive;
@@ -206,6 +215,8 @@ struct RowArgs {
 // value rows, the f32 strategy sums.
 struct Row64Args {
   const float* sums;
+  const uint16_t* sq;     // compressed storage: u16 sums and per-node scales (sums is null)
+  const float* sscale;
   double* reach;
   double* vals;
   uint32_t* alive;

@@ -34,11 +34,62 @@ __device__ __forceinline__ T pick(int q, const T (&v)[2]) {
 
 __device__ __forceinline__ bool nz4(const float4& v) { return v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f; }
 
+// ------------------------------------------------- 16-bit compressed storage
+// Storage::Compressed (storage.rs:87-330): per decision node, i16 regrets
+// scaled by rscale[slot] / 32767 and u16 strategy sums scaled by
+// sscale[slot] / 65535, where the node's scale is the max |value| of its
+// block after its last update. Regret matching reads the raw i16 values (a
+// positive scale cancels); every update decodes, updates in f32, takes the
+// block's new max and re-encodes. A block covers a whole row of the node, so
+// the max is a block reduction; every thread of the block must call it.
+__device__ __forceinline__ float4 ldq(const int16_t* p) {
+  const short4 q = *reinterpret_cast<const short4*>(p);
+  return make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+}
+__device__ __forceinline__ float4 ldq(const uint16_t* p) {
+  const ushort4 q = *reinterpret_cast<const ushort4*>(p);
+  return make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+}
+__device__ __forceinline__ float4 scale4(float4 v, float s) {
+  return make_float4(v.x * s, v.y * s, v.z * s, v.w * s);
+}
+__device__ __forceinline__ float absmax4(const float4& v) {
+  return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+}
+// Regret encoding (storage.rs:284-297): round half away from zero, then
+// Rust's saturating `as i16` (truncation toward zero).
+__device__ __forceinline__ int16_t enc_regret(float v, float inv) {
+  const float y = v * inv;
+  const float t = y + copysignf(0.5f, y);
+  return t >= 32767.0f ? (int16_t)32767 : t <= -32768.0f ? (int16_t)-32768 : (int16_t)__float2int_rz(t);
+}
+// Strategy-sum encoding (storage.rs:318-325): max(v, 0) * inv + 0.5,
+// saturating `as u16`.
+__device__ __forceinline__ uint16_t enc_sum(float v, float inv) {
+  const float t = fmaxf(v, 0.0f) * inv + 0.5f;
+  return t >= 65535.0f ? (uint16_t)65535 : (uint16_t)__float2uint_rz(t);
+}
+// Max over the block (all threads call it; blockDim a multiple of 32).
+__device__ __forceinline__ float block_max(float v) {
+  __shared__ float red[32];
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
+  __syncthreads();  // a previous call's reads of red are done
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float m = 0.0f;
+  const int nw = (int)(blockDim.x >> 5);
+  for (int w = 0; w < nw; w++) m = fmaxf(m, red[w]);
+  return m;
+}
+
 // ------------------------------------------------------------- down levels
 // Opponent split (cfr.rs:384-420 / river.rs:115-160) and chance split
 // (cfr.rs:448-456).
 // One warp's item: hands [h0, h0 + 128) of one node, 4 per lane.
-template <int MODE, int MAXA, int KIND>
+// COMP: compressed storage (T.cards holds the node's scale slot); the whole
+// block takes part in every call.
+template <int MODE, int MAXA, int KIND, bool COMP = false>
 __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, int h0, int lane) {
   const uint32_t live = A.alive[T.in_slot];
   if (live == 0) return;  // dead subtree: children stay dead
@@ -55,14 +106,33 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
     const float* base = (MODE == M_CFR ? A.regrets : A.sums) + T.store + h0;
     float* sb = A.sums + T.store + h0;
     float4 sums[MODE == M_CFR ? MAXA : 1];
+    // Compressed: the sums' decode factor (storage.rs:259-262, 313-314).
+    const float sdec = COMP ? A.sscale[T.cards] / 65535.0f : 0.0f;
     // Every storage load of the node is issued before the arithmetic.
-#pragma unroll
-    for (int a = 0; a < MAXA; a++)
-      if (a < na) x[a] = valid ? ld4(base + (size_t)a * hp) : make_float4(0.f, 0.f, 0.f, 0.f);
-    if (MODE == M_CFR) {
+    if constexpr (COMP) {
 #pragma unroll
       for (int a = 0; a < MAXA; a++)
-        if (a < na && valid) sums[a] = ld4(sb + (size_t)a * hp);
+        if (a < na) {
+          const size_t e = T.store + (size_t)a * hp + h0;
+          // CFR: raw i16 regrets (regret matching); otherwise the decoded sums.
+          x[a] = !valid ? make_float4(0.f, 0.f, 0.f, 0.f)
+                        : (MODE == M_CFR ? ldq(A.rq + e) : scale4(ldq(A.sq + e), sdec));
+        }
+      if (MODE == M_CFR) {
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na) sums[a] = valid ? scale4(ldq(A.sq + T.store + (size_t)a * hp + h0), sdec)
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) x[a] = valid ? ld4(base + (size_t)a * hp) : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (MODE == M_CFR) {
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na && valid) sums[a] = ld4(sb + (size_t)a * hp);
+      }
     }
     if (MODE == M_CFR) {
       // regret_match_into (cfr.rs:161-192).
@@ -81,6 +151,7 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
           for (int j = 0; j < VEC; j++) at(x[a], j) = at(inv, j) == 0.0f ? uniform : max0(at(x[a], j)) * at(inv, j);
       // Strategy sums s*gamma + sigma (or + sigma*reach) (cfr.rs:395-407).
       const DiscountD d = *A.disc;
+      float smax = 0.0f;
 #pragma unroll
       for (int a = 0; a < MAXA; a++)
         if (a < na && valid) {
@@ -90,8 +161,27 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
             float add = d.reach_weighted ? at(x[a], j) * at(r, j) : at(x[a], j);
             at(s, j) = at(s, j) * d.strat + add;
           }
-          st4(sb + (size_t)a * hp, s);
+          if constexpr (COMP) {
+            sums[MODE == M_CFR ? a : 0] = s;
+            smax = fmaxf(smax, absmax4(s));
+          } else {
+            st4(sb + (size_t)a * hp, s);
+          }
         }
+      if constexpr (COMP) {
+        // The node's new scale and the re-encoded sums (storage.rs:315-328).
+        const float mx = block_max(smax);
+        const float sinv = mx > 0.0f ? 65535.0f / mx : 0.0f;
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na && valid) {
+            const float4 s = sums[MODE == M_CFR ? a : 0];
+            ushort4 q = make_ushort4(0, 0, 0, 0);
+            if (mx > 0.0f) q = make_ushort4(enc_sum(s.x, sinv), enc_sum(s.y, sinv), enc_sum(s.z, sinv), enc_sum(s.w, sinv));
+            *reinterpret_cast<ushort4*>(A.sq + T.store + (size_t)a * hp + h0) = q;
+          }
+        if (threadIdx.x == 0) A.sscale[T.cards] = mx;
+      }
     } else {
       // normalize_in_place (cfr.rs:124-154).
 #pragma unroll
@@ -145,12 +235,81 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
 // --------------------------------------------------------------- up levels
 // Traverser node (own_node_update, cfr.rs:315-382), opponent node sum
 // (cfr.rs:421-432, river.rs:264-271) and chance sum (cfr.rs:462-478).
-template <int MODE, int MAXA, int KIND>
+// COMP: compressed storage (T.cards holds a traverser node's scale slot);
+// the whole block takes part in every call.
+template <int MODE, int MAXA, int KIND, bool COMP = false>
 __device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h0) {
   const uint32_t live = A.alive[T.slot];
   if (live == 0) return;
   const int p = A.p;
   const int hp = pick(p, A.hp);
+  if constexpr (COMP && KIND == U_OWN && MODE == M_CFR) {
+    // Compressed regret update (storage.rs:272-303 around
+    // own_node_update, cfr.rs:347-379): every thread reaches the block max.
+    const bool valid = h0 < hp;
+    const size_t stride = (size_t)A.stride;
+    const int na = (int)T.nchild;
+    const float rdec = A.rscale[T.cards] / 32767.0f;
+    float4 cfv[MAXA], r[MAXA];
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) {
+        cfv[a] = valid ? ld4(A.vals + (size_t)(T.child + a) * stride + h0) : z;
+        r[a] = valid ? scale4(ldq(A.rq + T.store + (size_t)a * hp + h0), rdec) : z;
+      }
+    const DiscountD d = *A.disc;
+    float4 out;
+#pragma unroll
+    for (int j = 0; j < VEC; j++) {
+      float s = max0(at(r[0], j));
+#pragma unroll
+      for (int a = 1; a < MAXA; a++)
+        if (a < na) s += max0(at(r[a], j));
+      float o = 0.0f;
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) o += max0(at(r[a], j)) * at(cfv[a], j);
+      float iv = recipf(s);
+      o *= iv;
+      if (iv == 0.0f) {
+        float m = -0.0f;
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na) m += at(cfv[a], j);
+        o = m * (1.0f / (float)na);
+      }
+      at(out, j) = o;
+    }
+    float rmax = 0.0f;
+#pragma unroll
+    for (int a = 0; a < MAXA; a++)
+      if (a < na) {
+#pragma unroll
+        for (int j = 0; j < VEC; j++) {
+          float x = at(r[a], j);
+          float disc = x > 0.0f ? d.pos : d.neg;
+          at(r[a], j) = x * disc + at(cfv[a], j) - at(out, j);
+        }
+        if (valid) rmax = fmaxf(rmax, absmax4(r[a]));
+      }
+    const float mx = block_max(rmax);
+    const float rinv = mx > 0.0f ? 32767.0f / mx : 0.0f;
+    if (valid) {
+#pragma unroll
+      for (int a = 0; a < MAXA; a++)
+        if (a < na) {
+          short4 q = make_short4(0, 0, 0, 0);
+          if (mx > 0.0f)
+            q = make_short4(enc_regret(r[a].x, rinv), enc_regret(r[a].y, rinv), enc_regret(r[a].z, rinv),
+                            enc_regret(r[a].w, rinv));
+          *reinterpret_cast<short4*>(A.rq + T.store + (size_t)a * hp + h0) = q;
+        }
+      st4(A.vals + (size_t)T.node * stride + h0, out);
+    }
+    if (threadIdx.x == 0) A.rscale[T.cards] = mx;
+    return;
+  }
   if (h0 >= hp) return;
   const size_t stride = (size_t)A.stride;
   float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -165,9 +324,17 @@ __device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h
     for (int a = 0; a < MAXA; a++)
       if (a < na) cfv[a] = ld4(A.vals + (size_t)(T.child + a) * stride + h0);
     if (MODE != M_BR) {
+      if constexpr (COMP) {
+        // Average mode: the decoded strategy sums (the CFR update is above).
+        const float sdec = A.sscale[T.cards] / 65535.0f;
 #pragma unroll
-      for (int a = 0; a < MAXA; a++)
-        if (a < na) st[MODE == M_BR ? 0 : a] = ld4(sbase + (size_t)a * hp);
+        for (int a = 0; a < MAXA; a++)
+          if (a < na) st[MODE == M_BR ? 0 : a] = scale4(ldq(A.sq + T.store + (size_t)a * hp + h0), sdec);
+      } else {
+#pragma unroll
+        for (int a = 0; a < MAXA; a++)
+          if (a < na) st[MODE == M_BR ? 0 : a] = ld4(sbase + (size_t)a * hp);
+      }
     }
     if (MODE == M_BR) {
       out = cfv[0];

@@ -38,6 +38,7 @@ EXPORTS = [
     "dcfr_mlp_forward", "dcfr_mlp_gradients", "dcfr_mlp_train_step",
     "dcfr_mlp_backward", "dcfr_mlp_gradients_device", "dcfr_mlp_adam_step", "dcfr_gemm_bf16", "dcfr_gemm_bf16_timed",
     "dcfr_create_depth_limited", "dcfr_node_storage", "dcfr_write_node",
+    "dcfr_storage_slots", "dcfr_download_storage_compressed", "dcfr_upload_storage_compressed",
 ]
 
 
@@ -92,6 +93,9 @@ def lib():
         L.dcfr_storage_len.argtypes = [P, C.POINTER(C.c_uint64)]
         L.dcfr_download_storage.argtypes = [P, P, P, C.c_uint64]
         L.dcfr_upload_storage.argtypes = [P, P, P, C.c_uint64]
+        L.dcfr_storage_slots.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.dcfr_download_storage_compressed.argtypes = [P, P, P, P, P, C.c_uint64, C.c_uint64]
+        L.dcfr_upload_storage_compressed.argtypes = [P, P, P, P, P, C.c_uint64, C.c_uint64]
         L.dcfr_set_iterations.argtypes = [P, C.c_uint32]
         L.dcfr_traverse.argtypes = [P, C.c_int32, C.c_int32, C.c_uint32, P]
         L.dcfr_kernel_launches.argtypes = [P, C.POINTER(C.c_uint64)]
@@ -420,6 +424,29 @@ class Solver:
                 raise ValueError("out arrays must be contiguous")
         check(lib().dcfr_download_storage(self._h, _ptr(r), _ptr(s), n))
         return r, s
+
+    def storage_slots(self) -> int:
+        n = C.c_uint64()
+        check(lib().dcfr_storage_slots(self._h, C.byref(n)))
+        return n.value
+
+    def download_storage_compressed(self):
+        """Compressed storage (storage.rs:92-97): i16 regrets, u16 sums and
+        the per-slot scales."""
+        n, k = self.storage_len(), self.storage_slots()
+        rq = np.zeros(n, np.int16)
+        sq = np.zeros(n, np.uint16)
+        rs = np.zeros(k, np.float32)
+        ss = np.zeros(k, np.float32)
+        check(lib().dcfr_download_storage_compressed(self._h, _ptr(rq), _ptr(sq), _ptr(rs), _ptr(ss), n, k))
+        return rq, sq, rs, ss
+
+    def upload_storage_compressed(self, rq, sq, rs, ss):
+        rq = np.ascontiguousarray(rq, np.int16)
+        sq = np.ascontiguousarray(sq, np.uint16)
+        rs = np.ascontiguousarray(rs, np.float32)
+        ss = np.ascontiguousarray(ss, np.float32)
+        check(lib().dcfr_upload_storage_compressed(self._h, _ptr(rq), _ptr(sq), _ptr(rs), _ptr(ss), len(rq), len(rs)))
 
     def upload_storage(self, regrets, sums):
         r = np.ascontiguousarray(regrets, np.float32)
