@@ -74,7 +74,14 @@ def workload_config(name: str, precision: str):
            "batch": workloads.river_spot, "learned": workloads.flop_spot}[name]()
     from poker_trainer_b200 import abi
     cfg.precision = abi.PRECISIONS[precision]
+    if STORAGE == "compressed":
+        cfg.storage = abi.STORAGE_COMPRESSED
     return cfg
+
+
+# --storage: the workloads' own f32 storage, or 16-bit compressed storage
+# (Storage::Compressed) on the same trees.
+STORAGE = "f32"
 
 
 # ----------------------------------------------------------------- CPU oracle
@@ -348,6 +355,7 @@ def run_ours(args, world, rank, local):
         "dtype": "f32", "data": "synthetic",
         "config": {
             "workload": WORKLOADS[args.workload], "iterations_per_step": 1, "precision": args.precision,
+            "storage": args.storage,
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "l2": (f"inputs larger than L2: one iteration moves {working / 1e6:.0f} MB of rows and storage "
                    f"(> {L2_BYTES / 1e6:.0f} MB L2), no flush") if working > L2_BYTES else
@@ -449,7 +457,8 @@ def run_flop(args, world, rank, local):
         "metric": METRIC, "value": K / (ms / 1000.0), "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS["flop"], "precision": args.precision, "parallelism": "single GPU",
+        "config": {"workload": WORKLOADS["flop"], "precision": args.precision, "storage": args.storage,
+                   "parallelism": "single GPU",
                    "l2": f"inputs larger than L2: one iteration moves {it_bytes / 1e9:.1f} GB"},
         "time_to_target": {"seconds": t_solve, "iterations": prog.iteration, "checks": len(checks),
                            "exploitability_pct": prog.exploitability_pct, "target_pct": 0.5,
@@ -743,6 +752,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="turn")
     ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--storage", choices=["f32", "compressed"], default="f32",
+                    help="turn, river, flop: f32 (the workloads' storage) or 16-bit compressed storage")
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -758,6 +769,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    global STORAGE
+    STORAGE = args.storage
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return run_reference(args, world, rank)

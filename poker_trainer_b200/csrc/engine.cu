@@ -217,10 +217,11 @@ int Engine::isomorphic_pairs() const {
 
 // Algorithmic bytes of one DCFR iteration: every decision node is once the
 // traverser's (regret read + write) and once the opponent's (regret read,
-// strategy-sum read + write): 20 B per storage cell; plus, per traversal,
-// one opponent-reach row read and one value row write per node.
+// strategy-sum read + write): 20 B per storage cell in f32, 10 B with 16-bit
+// storage; plus, per traversal, one opponent-reach row read and one value
+// row write per node.
 double Engine::iteration_bytes() const {
-  double cells = (double)g.storage_len;
+  double cells = (double)g.storage_len * (compressed_ ? 0.5 : 1.0);
   double nodes = (double)g.nodes.size();
   return 20.0 * cells + 2.0 * nodes * 4.0 * ((double)g.n[0] + (double)g.n[1]);
 }
@@ -861,12 +862,16 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   const double np_ = g.n[p], no_ = g.n[o];
   for (const std::vector<DownTask>* v : {&plan.h_down, &plan.h_fdown})
     for (const DownTask& t : *v)
-      plan.class_bytes[DCFR_KERNEL_DOWN] += (t.kind & KIND_MASK) == D_OPP_SPLIT ? 4.0 * no_ * (1.0 + 4.0 * t.nchild)
-                                                                                : 4.0 * no_ * (1.0 + t.nchild);
+      // Opponent split: reach row in, k rows out, regrets read, sums read and
+      // written (2-byte values with compressed storage).
+      plan.class_bytes[DCFR_KERNEL_DOWN] += (t.kind & KIND_MASK) == D_OPP_SPLIT
+                                                ? 4.0 * no_ * (1.0 + t.nchild) + (compressed_ ? 6.0 : 12.0) * no_ * t.nchild
+                                                : 4.0 * no_ * (1.0 + t.nchild);
   for (const std::vector<UpTask>* v : {&plan.h_up, &plan.h_fup})
     for (const UpTask& t : *v)
-      plan.class_bytes[DCFR_KERNEL_UP] +=
-          t.kind == U_OWN ? 4.0 * np_ * (3.0 * t.nchild + 1.0) : 4.0 * np_ * (t.nchild + 1.0);
+      plan.class_bytes[DCFR_KERNEL_UP] += t.kind == U_OWN
+                                              ? 4.0 * np_ * (t.nchild + 1.0) + (compressed_ ? 4.0 : 8.0) * np_ * t.nchild
+                                              : 4.0 * np_ * (t.nchild + 1.0);
   // Per terminal: one reach row read, one value row written, and the paired
   // fold's row.
   for (const FastTask& t : plan.h_fast)
