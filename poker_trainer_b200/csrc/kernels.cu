@@ -34,7 +34,8 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) down_kernel(RowArgs A, const 
   const DownTask T = tasks[t];  // plan data: readable before the wait
   pdl_wait();
   const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
-  if (T.kind == D_OPP_SPLIT) down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, threadIdx.x & 31);
+  int phase = 0;  // block_max scratch row (compressed storage)
+  if (T.kind == D_OPP_SPLIT) down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, threadIdx.x & 31, &phase);
   else down_item<MODE, 1, D_CHANCE_SPLIT>(A, T, h0, threadIdx.x & 31);
   pdl_launch_dependents();
 }
@@ -45,7 +46,8 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) up_kernel(RowArgs A, const Up
   const UpTask T = tasks[t];
   pdl_wait();
   const int h0 = (ch * (int)blockDim.x + (int)threadIdx.x) * VEC;
-  if (T.kind == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0);
+  int phase = 0;  // block_max scratch row (compressed storage)
+  if (T.kind == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0, &phase);
   else if (T.kind == U_OPP_SUM) up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
   else up_item<MODE, 1, U_CHANCE_SUM>(A, T, h0);
   pdl_launch_dependents();
@@ -61,11 +63,12 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_down_kernel(RowArgs A, 
   const FusedTree F = trees[blockIdx.x];
   pdl_wait();
   const int h0 = (int)threadIdx.x * VEC, lane = threadIdx.x & 31;
+  int phase = 0;  // block_max scratch row (compressed storage)
 #pragma unroll 1
   for (uint32_t i = 0; i < F.down_count; i++) {
     const DownTask T = tasks[F.down_first + i];
     if (T.kind & LEVEL_BREAK) __syncthreads();
-    down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, lane);
+    down_item<MODE, MAXA, D_OPP_SPLIT, COMP>(A, T, h0, lane, &phase);
   }
   pdl_launch_dependents();
 }
@@ -76,10 +79,11 @@ __global__ void __launch_bounds__(ROW_MAX_THREADS) fused_up_kernel(RowArgs A, co
   const FusedTree F = trees[blockIdx.x];
   pdl_wait();
   const int h0 = (int)threadIdx.x * VEC;
+  int phase = 0;  // block_max scratch row (compressed storage)
 #pragma unroll 1
   for (uint32_t i = 0; i < F.up_count; i++) {
     const UpTask T = tasks[F.up_first + i];
-    if ((T.kind & KIND_MASK) == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0);
+    if ((T.kind & KIND_MASK) == U_OWN) up_item<MODE, MAXA, U_OWN, COMP>(A, T, h0, &phase);
     else up_item<MODE, MAXA, U_OPP_SUM>(A, T, h0);
   }
   pdl_launch_dependents();

@@ -69,17 +69,22 @@ __device__ __forceinline__ uint16_t enc_sum(float v, float inv) {
   const float t = fmaxf(v, 0.0f) * inv + 0.5f;
   return t >= 65535.0f ? (uint16_t)65535 : (uint16_t)__float2uint_rz(t);
 }
-// Max over the block (all threads call it; blockDim a multiple of 32).
-__device__ __forceinline__ float block_max(float v) {
-  __shared__ float red[32];
+// Max over the block (all threads call it, in the same order; blockDim a
+// multiple of 32). Calls alternate between two scratch rows (`phase`, one
+// counter per thread that every thread advances alike), so one barrier per
+// call suffices: a row is rewritten only after the next call's barrier,
+// which every thread passes after its reads of that row.
+__device__ __forceinline__ float block_max(float v, int& phase) {
+  __shared__ float red[2][32];
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
-  __syncthreads();  // a previous call's reads of red are done
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  float* row = red[phase & 1];
+  phase++;
+  if ((threadIdx.x & 31) == 0) row[threadIdx.x >> 5] = v;
   __syncthreads();
   float m = 0.0f;
   const int nw = (int)(blockDim.x >> 5);
-  for (int w = 0; w < nw; w++) m = fmaxf(m, red[w]);
+  for (int w = 0; w < nw; w++) m = fmaxf(m, row[w]);
   return m;
 }
 
@@ -90,7 +95,7 @@ __device__ __forceinline__ float block_max(float v) {
 // COMP: compressed storage (T.cards holds the node's scale slot); the whole
 // block takes part in every call.
 template <int MODE, int MAXA, int KIND, bool COMP = false>
-__device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, int h0, int lane) {
+__device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, int h0, int lane, int* phase = nullptr) {
   const uint32_t live = A.alive[T.in_slot];
   if (live == 0) return;  // dead subtree: children stay dead
   const int o = A.p ^ 1;
@@ -170,7 +175,7 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
         }
       if constexpr (COMP) {
         // The node's new scale and the re-encoded sums (storage.rs:315-328).
-        const float mx = block_max(smax);
+        const float mx = block_max(smax, *phase);
         const float sinv = mx > 0.0f ? 65535.0f / mx : 0.0f;
 #pragma unroll
         for (int a = 0; a < MAXA; a++)
@@ -238,7 +243,7 @@ __device__ __forceinline__ void down_item(const RowArgs& A, const DownTask& T, i
 // COMP: compressed storage (T.cards holds a traverser node's scale slot);
 // the whole block takes part in every call.
 template <int MODE, int MAXA, int KIND, bool COMP = false>
-__device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h0) {
+__device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h0, int* phase = nullptr) {
   const uint32_t live = A.alive[T.slot];
   if (live == 0) return;
   const int p = A.p;
@@ -293,7 +298,7 @@ __device__ __forceinline__ void up_item(const RowArgs& A, const UpTask& T, int h
         }
         if (valid) rmax = fmaxf(rmax, absmax4(r[a]));
       }
-    const float mx = block_max(rmax);
+    const float mx = block_max(rmax, *phase);
     const float rinv = mx > 0.0f ? 32767.0f / mx : 0.0f;
     if (valid) {
 #pragma unroll
