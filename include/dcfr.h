@@ -41,7 +41,7 @@ enum {
   DCFR_ERR_INVALID_ARG = 5,   /* malformed config, NULL pointer, short buffer */
   DCFR_ERR_CUDA = 6,          /* a CUDA runtime call failed */
   DCFR_ERR_OUT_OF_MEMORY = 7, /* device memory exhausted */
-  DCFR_ERR_UNSUPPORTED = 8,   /* option not built (e.g. sampled chance) */
+  DCFR_ERR_UNSUPPORTED = 8,   /* option not built for this solver kind */
   DCFR_ERR_DEVICE_TIMEOUT = 9 /* a bounded device-side wait gave up */
 };
 
@@ -63,6 +63,13 @@ enum { DCFR_STORAGE_F32 = 0, DCFR_STORAGE_COMPRESSED = 1, DCFR_STORAGE_AUTO = 2 
  * rare one-rounding-step differences; EXACT sweeps in the CPU's f64
  * operation order and is bit-identical to the CPU solver. */
 enum { DCFR_PRECISION_FAST = 0, DCFR_PRECISION_EXACT = 1 };
+
+/* Chance modes (ChanceMode, crates/solver/src/tree.rs:128-136). SAMPLED deals
+ * a stratified sample of chance_turn turn cards and chance_river river cards
+ * per chance node (sample_cards, crates/solver/src/sampling.rs:9-54), drawn
+ * from rand 0.9's StdRng seeded with chance_seed; all-in runouts stay
+ * exact. */
+enum { DCFR_CHANCE_EXACT = 0, DCFR_CHANCE_SAMPLED = 1 };
 
 /* Traversal modes (cfr::Mode, crates/solver/src/cfr.rs:248-256). */
 enum { DCFR_MODE_CFR = 0, DCFR_MODE_BEST_RESPONSE = 1, DCFR_MODE_AVERAGE = 2 };
@@ -148,7 +155,10 @@ typedef struct dcfr_config {
   int32_t isomorphism;
   dcfr_params dcfr;
   int32_t precision; /* DCFR_PRECISION_* (Solver::use_gpu(precision), lib.rs:508-530) */
-  int32_t _pad4;
+  int32_t chance;    /* DCFR_CHANCE_* (SolveConfig::chance, lib.rs:88) */
+  int32_t chance_turn;
+  int32_t chance_river;
+  uint64_t chance_seed;
 } dcfr_config;
 
 /* TreeStats (crates/solver/src/tree.rs:248-257). */

@@ -72,6 +72,10 @@ static SolveConfig to_config(const dcfr_config* c) {
   cfg.dcfr.gamma = c->dcfr.gamma;
   cfg.dcfr.restart_average = c->dcfr.restart_average != 0;
   cfg.dcfr.unweighted_average = c->dcfr.unweighted_average != 0;
+  cfg.sampled = c->chance == DCFR_CHANCE_SAMPLED;
+  cfg.sample_turn = (size_t)c->chance_turn;
+  cfg.sample_river = (size_t)c->chance_river;
+  cfg.sample_seed = c->chance_seed;
   return cfg;
 }
 
@@ -85,6 +89,22 @@ static std::vector<Step> to_path(const dcfr_step* path, size_t n) {
 extern "C" {
 
 const char* oracle_last_error(void) { return g_err.c_str(); }
+
+// The sampled chance mode's pieces, for the tests that pin them.
+void oracle_chacha_block(const uint32_t key[8], uint64_t counter, uint64_t stream, int rounds, uint32_t out[16]) {
+  chacha_block(key, counter, stream, rounds, out);
+}
+void oracle_rng_u64(uint64_t seed, uint64_t n, uint64_t* out) {
+  ChaChaRng r(seed);
+  for (uint64_t i = 0; i < n; i++) out[i] = r.next_u64();
+}
+int oracle_sample_cards(const int32_t* available, int32_t n, int32_t k, uint64_t seed, int32_t* out) {
+  ChaChaRng r(seed);
+  std::vector<int> a(available, available + n);
+  std::vector<int> picks = sample_cards(a, (size_t)k, r);
+  for (size_t i = 0; i < picks.size(); i++) out[i] = picks[i];
+  return (int)picks.size();
+}
 void oracle_set_threads(int n) { set_num_threads(n); }
 int oracle_get_threads(void) { return get_num_threads(); }
 

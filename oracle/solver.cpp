@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <unordered_map>
 
 namespace oracle {
@@ -336,6 +337,124 @@ void StrengthTable::build(const HandSet& hands, const std::vector<int>& board) {
   }
 }
 
+// ---------------------------------------------------------------- sampling
+static inline uint32_t rotl32(uint32_t v, int n) { return (v << n) | (v >> (32 - n)); }
+
+void chacha_block(const uint32_t key[8], uint64_t counter, uint64_t stream, int rounds, uint32_t out[16]) {
+  // "expand 32-byte k"
+  const uint32_t init[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
+                             key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7],
+                             (uint32_t)(counter & 0xffffffffu), (uint32_t)(counter >> 32),
+                             (uint32_t)(stream & 0xffffffffu), (uint32_t)(stream >> 32)};
+  uint32_t x[16];
+  std::memcpy(x, init, sizeof x);
+  auto qr = [&x](int a, int b, int c, int d) {
+    x[a] += x[b];
+    x[d] ^= x[a];
+    x[d] = rotl32(x[d], 16);
+    x[c] += x[d];
+    x[b] ^= x[c];
+    x[b] = rotl32(x[b], 12);
+    x[a] += x[b];
+    x[d] ^= x[a];
+    x[d] = rotl32(x[d], 8);
+    x[c] += x[d];
+    x[b] ^= x[c];
+    x[b] = rotl32(x[b], 7);
+  };
+  for (int i = 0; i < rounds / 2; i++) {
+    // column round, then diagonal round
+    qr(0, 4, 8, 12);
+    qr(1, 5, 9, 13);
+    qr(2, 6, 10, 14);
+    qr(3, 7, 11, 15);
+    qr(0, 5, 10, 15);
+    qr(1, 6, 11, 12);
+    qr(2, 7, 8, 13);
+    qr(3, 4, 9, 14);
+  }
+  for (int i = 0; i < 16; i++) out[i] = x[i] + init[i];
+}
+
+ChaChaRng::ChaChaRng(uint64_t state) {
+  // seed_from_u64: eight PCG32 steps, each output one little-endian key word.
+  const uint64_t MUL = 6364136223846793005ull, INC = 11634580027462260723ull;
+  for (int i = 0; i < 8; i++) {
+    state = state * MUL + INC;
+    uint32_t xorshifted = (uint32_t)(((state >> 18) ^ state) >> 27);
+    uint32_t rot = (uint32_t)(state >> 59);
+    key[i] = rot == 0 ? xorshifted : (xorshifted >> rot) | (xorshifted << (32 - rot));
+  }
+}
+
+uint64_t ChaChaRng::next_u64() {
+  // BlockRng::next_u64: two words, low first; a pair that straddles the
+  // buffer end takes the last word and the first of the next buffer.
+  auto generate = [this]() {
+    for (int b = 0; b < 4; b++) chacha_block(key, block_counter + (uint64_t)b, 0, 12, results + 16 * b);
+    block_counter += 4;
+  };
+  if (index < 63) {
+    uint64_t v = (uint64_t)results[index] | ((uint64_t)results[index + 1] << 32);
+    index += 2;
+    return v;
+  }
+  if (index >= 64) {
+    generate();
+    index = 2;
+    return (uint64_t)results[0] | ((uint64_t)results[1] << 32);
+  }
+  uint64_t lo = results[63];
+  generate();
+  index = 1;
+  return lo | ((uint64_t)results[0] << 32);
+}
+
+double ChaChaRng::random_f64() {
+  const double scale = 1.0 / (double)(1ull << 53);
+  return scale * (double)(next_u64() >> (64 - 53));
+}
+
+std::vector<int> sample_cards(const std::vector<int>& available, size_t k, ChaChaRng& rng) {
+  if (k >= available.size()) return available;
+  std::vector<int> by_suit[4];
+  for (int c : available) by_suit[card_suit(c)].push_back(c);
+  for (auto& v : by_suit)
+    std::sort(v.begin(), v.end(), [](int a, int b) { return card_rank(a) < card_rank(b); });
+  double total = (double)available.size();
+  size_t quotas[4] = {0, 0, 0, 0};
+  std::vector<std::tuple<double, double, size_t>> fracs;
+  for (size_t s = 0; s < 4; s++) {
+    double exact = (double)k * (double)by_suit[s].size() / total;
+    quotas[s] = (size_t)std::floor(exact);
+    fracs.emplace_back(exact - std::floor(exact), rng.random_f64(), s);
+  }
+  size_t assigned = quotas[0] + quotas[1] + quotas[2] + quotas[3];
+  std::sort(fracs.begin(), fracs.end(), [](const auto& a, const auto& b) { return b < a; });
+  for (auto& f : fracs) {
+    if (assigned >= k) break;
+    size_t s = std::get<2>(f);
+    if (quotas[s] < by_suit[s].size()) {
+      quotas[s] += 1;
+      assigned += 1;
+    }
+  }
+  std::vector<int> out;
+  for (size_t s = 0; s < 4; s++) {
+    size_t m = by_suit[s].size(), q = quotas[s];
+    if (q == 0) continue;
+    double step = (double)m / (double)q;
+    double offset = rng.random_f64() * step;
+    for (size_t j = 0; j < q; j++) {
+      size_t idx = std::min((size_t)std::floor(offset + (double)j * step), m - 1);
+      out.push_back(by_suit[s][idx]);
+    }
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return out;
+}
+
 // ---------------------------------------------------------------- tree
 struct TreeParams {
   Street root_street;
@@ -346,6 +465,9 @@ struct TreeParams {
   size_t num_hands[2];
   double rake_rate, rake_cap;
   const Isomorphism* iso;
+  bool sampled = false;
+  size_t sample_turn = 0, sample_river = 0;
+  ChaChaRng* rng = nullptr;  // the builder's (or the count's) generator
 
   const PostflopMenu& menu_for(Street s) const { return s == root_street ? *menu : *future_menu; }
   std::vector<Action> actions(const BettingState& st) const {
@@ -353,9 +475,14 @@ struct TreeParams {
   }
   // tree.rs:310-312.
   float rake(Chips pot) const { return (float)std::min((double)pot * rake_rate, rake_cap); }
-  // tree.rs:315-334 (exact chance mode).
-  void chance_cards(const std::vector<int>& dealt, std::vector<int>& canon, std::vector<IsoRef>& refs,
-                    size_t& n_avail) const {
+  // tree.rs:302-308.
+  size_t sample_size(Street next, bool& has) const {
+    has = sampled;
+    return next == TURN ? sample_turn : sample_river;
+  }
+  // tree.rs:315-334.
+  void chance_cards(const std::vector<int>& dealt, bool all_in, Street next, std::vector<int>& canon,
+                    std::vector<IsoRef>& refs, size_t& n_avail) const {
     std::vector<int> board = *root_board;
     board.insert(board.end(), dealt.begin(), dealt.end());
     uint64_t used = 0;
@@ -364,6 +491,13 @@ struct TreeParams {
     for (int c = 0; c < 52; c++)
       if (!(used >> c & 1)) available.push_back(c);
     n_avail = available.size();
+    bool has;
+    size_t k = sample_size(next, has);
+    if (!all_in && has && k < n_avail) {
+      canon = sample_cards(available, k, *rng);
+      refs.clear();
+      return;
+    }
     iso->chance_cards(board, available, canon, refs);
   }
 };
@@ -401,7 +535,7 @@ static void count_after_street(const TreeParams& params, const BettingState& st,
   std::vector<int> cards;
   std::vector<IsoRef> refs;
   size_t n_avail;
-  params.chance_cards(dealt, cards, refs, n_avail);
+  params.chance_cards(dealt, all_in, next, cards, refs, n_avail);
   bool uniform = refs.empty() && !params.iso->enabled;
   size_t nreps = uniform ? 1 : cards.size();
   TreeStats sub;
@@ -527,7 +661,7 @@ struct Builder {
     std::vector<int> cards;
     std::vector<IsoRef> refs;
     size_t n_avail;
-    params.chance_cards(dealt, cards, refs, n_avail);
+    params.chance_cards(dealt, all_in, next, cards, refs, n_avail);
     size_t board_len = params.root_board->size() + dealt.size();
     float compatible = (float)(52 - board_len - 4);
     size_t total_cards = cards.size() + refs.size();
@@ -1495,6 +1629,9 @@ static TreeParams make_params(const SolveConfig& cfg, const HandSet& hands, cons
   tp.rake_rate = cfg.rake_rate;
   tp.rake_cap = cfg.rake_cap;
   tp.iso = &iso;
+  tp.sampled = cfg.sampled;
+  tp.sample_turn = cfg.sample_turn;
+  tp.sample_river = cfg.sample_river;
   return tp;
 }
 
@@ -1512,6 +1649,8 @@ bool Solver::estimate(const SolveConfig& cfg, TreeStats& out, int& err, std::str
   TreeParams tp = make_params(cfg, hands, iso);
   TreeStats st;
   std::vector<int> dealt;
+  ChaChaRng count_rng(0);  // count_tree's own generator (tree.rs:338-343)
+  tp.rng = &count_rng;
   count_player(tp, cfg.root, dealt, st);
   st.compressed = compressed_mode(cfg, st);
   out = st;
@@ -1526,6 +1665,8 @@ std::unique_ptr<Solver> Solver::create(const SolveConfig& cfg, int& err, std::st
   TreeParams tp = make_params(s->config, s->hands, s->iso);
   TreeStats st;
   std::vector<int> dealt;
+  ChaChaRng count_rng(0);  // count_tree's own generator (tree.rs:338-343)
+  tp.rng = &count_rng;
   count_player(tp, s->config.root, dealt, st);
   st.compressed = compressed_mode(s->config, st);
   uint64_t needed = st.memory_bytes();
@@ -1537,6 +1678,8 @@ std::unique_ptr<Solver> Solver::create(const SolveConfig& cfg, int& err, std::st
     msg = buf;
     return nullptr;
   }
+  ChaChaRng build_rng(s->config.sampled ? s->config.sample_seed : 0);  // Builder::new (tree.rs:415-420)
+  tp.rng = &build_rng;
   Builder b(tp);
   b.build(s->config.root);
   s->tree = std::move(b.tree);

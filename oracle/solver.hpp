@@ -81,7 +81,31 @@ struct SolveConfig {
   int storage = STORAGE_AUTO;
   bool isomorphism = true;
   DcfrParams dcfr;
+  // ChanceMode (tree.rs:128-136): sampled = false is Exact.
+  bool sampled = false;
+  size_t sample_turn = 0, sample_river = 0;
+  uint64_t sample_seed = 0;
 };
+
+// rand 0.9.5 StdRng = rand_chacha 0.9.0 ChaCha12Rng behind rand_core 0.9's
+// BlockRng (a 64-word buffer of four ChaCha blocks), seeded by
+// SeedableRng::seed_from_u64 (PCG32 key expansion). Restated from the
+// published ChaCha and PCG32 algorithms; tree.rs:415-420 and
+// sampling.rs:9-54 are its call sites.
+struct ChaChaRng {
+  uint32_t key[8];
+  uint64_t block_counter = 0;
+  uint32_t results[64];
+  size_t index = 64;
+  explicit ChaChaRng(uint64_t seed);
+  uint64_t next_u64();
+  double random_f64();  // StandardUniform for f64: [0, 1), 53 bits
+};
+// The ChaCha block function with `rounds` rounds (20 for ChaCha20, 12 for
+// StdRng): key words 4-11, counter words 12-13, stream words 14-15.
+void chacha_block(const uint32_t key[8], uint64_t counter, uint64_t stream, int rounds, uint32_t out[16]);
+// sampling.rs:9-54.
+std::vector<int> sample_cards(const std::vector<int>& available, size_t k, ChaChaRng& rng);
 
 // TreeStats (tree.rs:248-274). Node is 56 bytes in the reference's layout
 // (tree.rs:154-171: 8+16+8+4+4+4+4+2+2+1 bytes, padded to 8).

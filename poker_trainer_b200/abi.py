@@ -31,6 +31,7 @@ FOLD, CHECK, CALL, RAISE = 0, 1, 2, 3
 STORAGE_F32, STORAGE_COMPRESSED, STORAGE_AUTO = 0, 1, 2
 PRECISION_FAST, PRECISION_EXACT = 0, 1  # GpuPrecision (crates/solver/src/gpu/mod.rs:51-63)
 PRECISIONS = {"fast": PRECISION_FAST, "exact": PRECISION_EXACT}
+CHANCE_EXACT, CHANCE_SAMPLED = 0, 1  # ChanceMode (crates/solver/src/tree.rs:128-136)
 MODE_CFR, MODE_BEST_RESPONSE, MODE_AVERAGE = 0, 1, 2
 
 
@@ -111,7 +112,10 @@ class Config(C.Structure):
         ("isomorphism", C.c_int32),
         ("dcfr", Params),
         ("precision", C.c_int32),
-        ("_pad4", C.c_int32),
+        ("chance", C.c_int32),
+        ("chance_turn", C.c_int32),
+        ("chance_river", C.c_int32),
+        ("chance_seed", C.c_uint64),
     ]
 
 
@@ -325,9 +329,11 @@ def make_config(board, ranges, *, root=None, pot=None, stack=None, menu_: Menu |
                 future_menu: Menu | None = None, big_blind=100, prune=0.0, keep=((), ()),
                 max_memory_bytes=8 << 30, rake_rate=0.0, rake_cap=0.0, storage=STORAGE_AUTO,
                 isomorphism=True, alpha=1.5, beta=0.0, beta_clip=False, gamma=3.0,
-                restart_average=True, unweighted_average=True, precision="fast") -> Config:
+                restart_average=True, unweighted_average=True, precision="fast",
+                sampled: tuple[int, int, int] | None = None) -> Config:
     """SolveConfig (crates/solver/src/lib.rs:74-135), defaults as
-    SolveConfig::new and DcfrParams::default (cfr.rs:72-80)."""
+    SolveConfig::new and DcfrParams::default (cfr.rs:72-80). `sampled` =
+    (turn, river, seed) selects ChanceMode::Sampled."""
     cfg = Config()
     cards = parse_cards(board) if isinstance(board, str) else list(board)
     if len(cards) > 5:
@@ -361,6 +367,9 @@ def make_config(board, ranges, *, root=None, pot=None, stack=None, menu_: Menu |
     cfg.dcfr.beta_clip = int(beta_clip)
     cfg.dcfr.restart_average, cfg.dcfr.unweighted_average = int(restart_average), int(unweighted_average)
     cfg.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    if sampled is not None:
+        cfg.chance = CHANCE_SAMPLED
+        cfg.chance_turn, cfg.chance_river, cfg.chance_seed = sampled
     return cfg
 
 

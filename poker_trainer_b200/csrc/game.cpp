@@ -1,5 +1,6 @@
 // Host-side game model of libdcfr (see game.hpp).
 #include "game.hpp"
+#include "chance_sample.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -174,6 +175,7 @@ struct Ctx {
   int root_street;
   int64_t bb;
   std::unordered_map<uint64_t, uint32_t> board_index;
+  StdRng* rng = nullptr;  // the sampled chance mode's generator
 
   const dcfr_menu& menu_for(int street) const { return street == root_street ? *menu : *future; }
   std::vector<Act> acts(const Betting& st) const { return state_actions(st, menu_for(st.street), bb); }
@@ -181,9 +183,12 @@ struct Ctx {
     return (float)std::min((double)pot * g->cfg.rake_rate, g->cfg.rake_cap);
   }
   // Canonical cards and isomorphic references dealt at a chance node
-  // (tree.rs:315-334, iso.rs:120-141).
-  void deal(const std::vector<int>& dealt, std::vector<int>& canon, std::vector<int>& iso_card,
-            std::vector<int>& iso_canon, std::vector<int>& iso_pair, int& n_avail) const {
+  // (tree.rs:315-334, iso.rs:120-141). In the sampled chance mode a chance
+  // node that is not an all-in runout deals a stratified sample of the
+  // street's size instead, with no isomorphic references.
+  void deal(const std::vector<int>& dealt, bool all_in, int next, std::vector<int>& canon,
+            std::vector<int>& iso_card, std::vector<int>& iso_canon, std::vector<int>& iso_pair,
+            int& n_avail) const {
     uint64_t used = 0;
     uint16_t m[4] = {0, 0, 0, 0};
     for (int c : g->board) {
@@ -198,6 +203,17 @@ struct Ctx {
     iso_card.clear();
     iso_canon.clear();
     iso_pair.clear();
+    n_avail = 52 - __builtin_popcountll(used);
+    if (g->cfg.chance == DCFR_CHANCE_SAMPLED && !all_in) {
+      const size_t k = (size_t)(next == DCFR_TURN ? g->cfg.chance_turn : g->cfg.chance_river);
+      if (k < (size_t)n_avail) {
+        std::vector<int> available;
+        for (int c = 0; c < 52; c++)
+          if (!(used >> c & 1)) available.push_back(c);
+        canon = sample_cards(available, k, *rng);
+        return;
+      }
+    }
     n_avail = 0;
     bool any = false;
     for (int i = 0; i < 6; i++) any |= g->sym[i];
@@ -252,7 +268,7 @@ static void count_street_over(Ctx& cx, const Betting& st, std::vector<int>& deal
   bool all_in = st.stack[0] == 0 || st.stack[1] == 0;
   std::vector<int> canon, ic, icn, ip;
   int n_avail;
-  cx.deal(dealt, canon, ic, icn, ip, n_avail);
+  cx.deal(dealt, all_in, st.street + 1, canon, ic, icn, ip, n_avail);
   bool uniform = ic.empty() && !cx.g->iso_enabled;
   size_t reps = uniform ? 1 : canon.size();
   Stats sub;
@@ -360,7 +376,7 @@ static void fill_street_over(Ctx& cx, uint32_t id, const Betting& st, int32_t i0
   bool all_in = st.stack[0] == 0 || st.stack[1] == 0;
   std::vector<int> canon, ic, icn, ip;
   int n_avail;
-  cx.deal(dealt, canon, ic, icn, ip, n_avail);
+  cx.deal(dealt, all_in, st.street + 1, canon, ic, icn, ip, n_avail);
   size_t board_len = g.board.size() + dealt.size();
   float compatible = (float)(52 - board_len - 4);
   size_t total_cards = canon.size() + ic.size();
@@ -547,6 +563,20 @@ int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tre
     msg = "root.to_act must be 0 or 1";
     return DCFR_ERR_INVALID_ARG;
   }
+  if (cfg.chance != DCFR_CHANCE_EXACT && cfg.chance != DCFR_CHANCE_SAMPLED) {
+    msg = "chance must be DCFR_CHANCE_EXACT or DCFR_CHANCE_SAMPLED";
+    return DCFR_ERR_INVALID_ARG;
+  }
+  if (cfg.chance == DCFR_CHANCE_SAMPLED) {
+    if (cfg.chance_turn < 1 || cfg.chance_river < 1) {
+      msg = "a sampled chance mode deals at least one card per street";
+      return DCFR_ERR_INVALID_ARG;
+    }
+    if (leaf_street >= 0) {
+      msg = "the depth-limited solver values every dealt card; the sampled chance mode is not built for it";
+      return DCFR_ERR_UNSUPPORTED;
+    }
+  }
   for (const dcfr_menu* m : {&cfg.menu, &cfg.future_menu}) {
     for (const dcfr_street_sizes* s : {&m->flop, &m->turn, &m->river})
       if (s->n_bet < 0 || s->n_bet > DCFR_MAX_SIZES || s->n_raise < 0 || s->n_raise > DCFR_MAX_SIZES) {
@@ -589,6 +619,11 @@ int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tre
   root.to_act = cfg.root.to_act;
   std::vector<int> dealt;
   g.stats = Stats();
+  // The count draws from its own generator seeded 0 (count_tree,
+  // tree.rs:338-343); the tree itself from one seeded with the configured
+  // seed (Builder::new, tree.rs:415-420).
+  StdRng count_rng(0);
+  cx.rng = &count_rng;
   count_player(cx, root, dealt, g.stats);
   // StorageMode (storage.rs:79-85, lib.rs:346-352).
   uint64_t f32_bytes = reference_memory_bytes(g.stats, false);
@@ -608,6 +643,8 @@ int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tre
   g.storage_len = 0;
   g.player_nodes = 0;
   g.nodes.push_back(GNode());
+  StdRng build_rng(cfg.chance_seed);
+  cx.rng = &build_rng;
   fill_player(cx, 0, root, 0, 0, dealt);
   return DCFR_OK;
 }

@@ -99,6 +99,12 @@ def lib():
         L.oracle_showdown_batch.argtypes = [P, C.c_int, C.c_int, P, P, P, P, P, P, P]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_get_threads.restype = C.c_int
+        L.oracle_chacha_block.argtypes = [P, C.c_uint64, C.c_uint64, C.c_int, P]
+        L.oracle_chacha_block.restype = None
+        L.oracle_rng_u64.argtypes = [C.c_uint64, C.c_uint64, P]
+        L.oracle_rng_u64.restype = None
+        L.oracle_sample_cards.argtypes = [P, C.c_int32, C.c_int32, C.c_uint64, P]
+        L.oracle_sample_cards.restype = C.c_int
         _lib = L
     return _lib
 
@@ -113,6 +119,29 @@ def parse_range(s: str) -> np.ndarray:
     if rc:
         raise ValueError(lib().oracle_last_error().decode())
     return out
+
+
+def chacha_block(key: np.ndarray, counter: int, stream: int, rounds: int) -> np.ndarray:
+    """One ChaCha block as 16 u32 words (the sampled chance mode's core)."""
+    key = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(16, np.uint32)
+    lib().oracle_chacha_block(ptr(key), counter, stream, rounds, ptr(out))
+    return out
+
+
+def rng_u64(seed: int, n: int) -> np.ndarray:
+    """The first n 64-bit draws of StdRng::seed_from_u64(seed)."""
+    out = np.zeros(n, np.uint64)
+    lib().oracle_rng_u64(seed, n, ptr(out))
+    return out
+
+
+def sample_cards(available, k: int, seed: int) -> list[int]:
+    """sampling.rs:9-54 with a fresh StdRng::seed_from_u64(seed)."""
+    a = np.ascontiguousarray(available, dtype=np.int32)
+    out = np.zeros(max(len(a), 1), np.int32)
+    n = lib().oracle_sample_cards(ptr(a), len(a), k, seed, ptr(out))
+    return [int(x) for x in out[:n]]
 
 
 def estimate(cfg: abi.Config) -> abi.TreeStats:

@@ -40,6 +40,36 @@ def allin_turn_config(**kw):
                   storage=abi.STORAGE_F32, **kw)
 
 
+def sampled_flop_config(**kw):
+    """tests.rs:151-170: a flop with ChanceMode::Sampled {turn: 8, river: 6,
+    seed: 3} and a one-size future menu."""
+    return config("Kh7d2c", "AK, KQ, 77, 22, AJs, QJs, T9s, 65s, A5s",
+                  "AK, KJ, QQ, JJ, 88, A7s, 98s, JTs, 76s", 600, 9700,
+                  future_menu=abi.menu(["66%"], ["3x"]), sampled=(8, 6, 3), **kw)
+
+
+def sampled_turn_config(seed=3, river=6, **kw):
+    """The turn spot of testutil.rs:79-89 with sampled rivers."""
+    return turn_config(sampled=(8, river, seed), **kw)
+
+
+def sampled_allin_turn_config(seed=5, **kw):
+    """The all-in turn spot (testutil.rs:108-118) with sampled rivers: the
+    pot-sized bet's all-in runouts stay exact, the checked-through rivers
+    are sampled."""
+    return allin_turn_config(sampled=(8, 5, seed), **kw)
+
+
+def sampled_iso_flop_config(seed=7, **kw):
+    """A flop with clubs and hearts interchangeable (the ranges of
+    testutil.rs:94-104 on Qs9s4d) and a short stack, sampled 6 turns and 4
+    rivers: all-in runouts stay exact and use isomorphism, so the tree's size
+    depends on which turn cards the sample drew."""
+    return config("Qs9s4d", "AQ, KQ, QJs, JTs, 99, 44, T9s, 87s, A5s, KJs, 65s",
+                  "AA, KK, AQ, QT, 99, JJ, TT, 98s, KJs, 65s, AJs, 33", 600, 1500,
+                  abi.menu(["100%"], ["3x"]), storage=abi.STORAGE_F32, sampled=(6, 4, seed), **kw)
+
+
 def facing_bet(pot, stack, bet):
     """testutil.rs:152-164."""
     return abi.betting_state(abi.RIVER, pot + bet, (0, bet), (stack, stack - bet), bet, bet, 1, 0, (True, False))

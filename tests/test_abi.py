@@ -99,6 +99,10 @@ CONFIGS = {
     "iso_turn": spots.iso_turn_config,
     "allin_turn": spots.allin_turn_config,
     "mid_street_raked": lambda: spots.mid_street_config(True),
+    "sampled_flop": spots.sampled_flop_config,
+    "sampled_turn": spots.sampled_turn_config,
+    "sampled_allin_turn": spots.sampled_allin_turn_config,
+    "sampled_iso_flop": spots.sampled_iso_flop_config,
 }
 
 
