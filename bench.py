@@ -76,12 +76,24 @@ def workload_config(name: str, precision: str):
     cfg.precision = abi.PRECISIONS[precision]
     if STORAGE == "compressed":
         cfg.storage = abi.STORAGE_COMPRESSED
+    if SAMPLE is not None:
+        cfg.chance = abi.CHANCE_SAMPLED
+        cfg.chance_turn, cfg.chance_river, cfg.chance_seed = SAMPLE
     return cfg
 
 
 # --storage: the workloads' own f32 storage, or 16-bit compressed storage
 # (Storage::Compressed) on the same trees.
 STORAGE = "f32"
+# --chance sampled: (turn cards, river cards, seed) of ChanceMode::Sampled on
+# the same spots; None deals every card.
+SAMPLE = None
+
+
+def chance_desc() -> str:
+    if SAMPLE is None:
+        return "exact"
+    return f"sampled: {SAMPLE[0]} turn and {SAMPLE[1]} river cards per chance node, seed {SAMPLE[2]}"
 
 
 # ----------------------------------------------------------------- CPU oracle
@@ -356,6 +368,7 @@ def run_ours(args, world, rank, local):
         "config": {
             "workload": WORKLOADS[args.workload], "iterations_per_step": 1, "precision": args.precision,
             "storage": args.storage,
+            "chance": chance_desc(),
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "l2": (f"inputs larger than L2: one iteration moves {working / 1e6:.0f} MB of rows and storage "
                    f"(> {L2_BYTES / 1e6:.0f} MB L2), no flush") if working > L2_BYTES else
@@ -458,7 +471,7 @@ def run_flop(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOADS["flop"], "precision": args.precision, "storage": args.storage,
-                   "parallelism": "single GPU",
+                   "chance": chance_desc(), "parallelism": "single GPU",
                    "l2": f"inputs larger than L2: one iteration moves {it_bytes / 1e9:.1f} GB"},
         "time_to_target": {"seconds": t_solve, "iterations": prog.iteration, "checks": len(checks),
                            "exploitability_pct": prog.exploitability_pct, "target_pct": 0.5,
@@ -754,6 +767,10 @@ def main():
     ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
     ap.add_argument("--storage", choices=["f32", "compressed"], default="f32",
                     help="turn, river, flop: f32 (the workloads' storage) or 16-bit compressed storage")
+    ap.add_argument("--chance", choices=["exact", "sampled"], default="exact",
+                    help="turn, river, flop: every card, or ChanceMode::Sampled with --sample")
+    ap.add_argument("--sample", default="8,6,3", metavar="TURN,RIVER,SEED",
+                    help="--chance sampled: cards dealt per turn and river chance node, and the seed")
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -769,8 +786,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
-    global STORAGE
+    global STORAGE, SAMPLE
     STORAGE = args.storage
+    if args.chance == "sampled":
+        t, r, sd = (int(x) for x in args.sample.split(","))
+        if t < 1 or r < 1:
+            ap.error("--sample deals at least one card per street")
+        SAMPLE = (t, r, sd)
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return run_reference(args, world, rank)
