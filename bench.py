@@ -654,7 +654,7 @@ def run_learned(args, world, rank, local):
     """Config of the learned depth-limited flop solve: data from the GPU
     solver, training on the library's tensor-core kernels, the depth-limited
     solve against the full-tree solve, and the depth-limited flop strategy
-    judged inside the full tree by the FP64 best-response oracle."""
+    evaluated inside the full tree by the FP64 best-response oracle."""
     import numpy as np
     import torch
     from poker_trainer_b200 import leafdata
@@ -696,7 +696,7 @@ def run_learned(args, world, rank, local):
     pd = dl.solve(opts)
     dl.synchronize()
     t_dl = time.perf_counter() - t0
-    # Judge: the depth-limited flop strategy inside the full tree.
+    # Check: the depth-limited flop strategy inside the full tree.
     paths = flop_paths(dl)
     diffs = []
     for path in paths:
@@ -708,7 +708,7 @@ def run_learned(args, world, rank, local):
         diffs.append(float(np.max(np.abs(rs(q.strategy) - rs(qf.strategy)))))
     e_comb, _ = full.exploitability_fp64()
     full.close()
-    # Judge 2: the depth-limited flop strategy locked into the full tree and
+    # Check 2: the depth-limited flop strategy locked into the full tree and
     # the turn and river re-solved around it. Its regrets are written as
     # 1e20 x its probabilities: regret matching keeps playing it exactly
     # (what one iteration adds is below f32 resolution of those regrets, and

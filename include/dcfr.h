@@ -282,7 +282,7 @@ int dcfr_node_storage(dcfr_solver* s, const dcfr_step* path, size_t n, uint64_t*
                       int32_t* num_hands);
 /* Overwrites the regrets and/or strategy sums (either may be NULL) of the
  * decision node at `path` from [num_actions][num_hands] blocks in the
- * reference layout; e.g. to judge a depth-limited solve's flop strategy
+ * reference layout; e.g. to evaluate a depth-limited solve's flop strategy
  * inside a full tree. */
 int dcfr_write_node(dcfr_solver* s, const dcfr_step* path, size_t n, const float* regrets, const float* sums);
 /* Solver::root_values (lib.rs:468-470): average-strategy EV of each player. */
