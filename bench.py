@@ -232,6 +232,20 @@ TERMINAL_KERNEL = {"turn": "fast_terminal_kernel", "turn-narrow": "warp_terminal
                    "river": "fast_terminal_kernel", "flop": "warp_terminal_kernel"}
 
 
+def spawn_ranks(n: int) -> int:
+    """--gpus N without a launcher: re-runs this command as N ranks, one
+    process per GPU (torch.distributed.run on 127.0.0.1), and returns its
+    exit status. Rank 0 prints the JSON line."""
+    import socket
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def dist_setup(n_gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -240,12 +254,65 @@ def dist_setup(n_gpus: int):
 
 
 # ----------------------------------------------------------------- arms
+def time_oracle_solve(cfg, threads: int, max_iterations: int, target_pct: float, check_every: int):
+    """Seconds of the oracle's solve (run_solve, lib.rs:594-642: DCFR
+    iterations with exploitability checks on the reference's schedule) from
+    a fresh solver to the target, wall clock; creation is not timed."""
+    from poker_trainer_b200 import abi
+    L = oracle_lib()
+    L.oracle_solve.argtypes = [C.c_void_p, C.POINTER(abi.SolveOptions), abi.PROGRESS_CB, C.c_void_p,
+                               C.POINTER(abi.Progress)]
+    L.oracle_set_threads(threads)
+    err = C.c_int(0)
+    h = L.oracle_create(C.byref(cfg), C.byref(err))
+    if not h:
+        raise RuntimeError(f"oracle_create failed ({err.value})")
+    checks = []
+
+    def cb(p, _u):
+        checks.append((p.contents.iteration, p.contents.exploitability_pct))
+        return 1
+
+    cbf = abi.PROGRESS_CB(cb)
+    opts = abi.SolveOptions(max_iterations, check_every, target_pct)
+    out = abi.Progress()
+    try:
+        t0 = time.perf_counter()
+        L.oracle_solve(h, C.byref(opts), cbf, None, C.byref(out))
+        secs = time.perf_counter() - t0
+    finally:
+        L.oracle_destroy(h)
+    return secs, out.iteration, out.exploitability_pct, checks, L.oracle_get_threads()
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
     from poker_trainer_b200 import abi  # noqa: F401  (config layout only)
     cfg = workload_config(args.workload, args.precision)
     threads = os.cpu_count() or 1
+    if args.workload == "flop":
+        secs, iters, pct, checks, used = time_oracle_solve(cfg, threads, args.max_iterations, 0.5, 10)
+        sample = (f"one full solve of the flop workload to 0.5% of the pot: {iters} DCFR iterations and "
+                  f"{len(checks)} exploitability checks on the reference's schedule (check every 10), ended at "
+                  f"{pct:.4f}%")
+        line = {
+            "impl": "reference", "metric": METRIC, "value": secs, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(iters, 1),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOADS["flop"], "parallelism": "host threads",
+                       "implementation": "CPU restatement of the reference's Rust solver (oracle/, C++ with OpenMP "
+                                         "over chance children); the Rust crate cannot be built here",
+                       "step": "one DCFR iteration of the solve; value is the wall time of the whole solve to 0.5% "
+                               "of the pot from a fresh solver (creation untimed)"},
+            "time_to_target": {"seconds": secs, "iterations": iters, "checks": len(checks),
+                               "exploitability_pct": pct, "target_pct": 0.5},
+            "checks": checks,
+            "cpu_baseline": {"value": secs, "unit": "s", "cores": used, "kind": "port", "sample": sample},
+            "e2e": {"value": secs, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return 0
     steps, secs, used = time_oracle(cfg, threads, args.warmup, args.steps, args.reference_budget_s)
     value = steps / secs
     sample = f"{steps} DCFR iterations after {args.warmup} untimed ({args.workload} workload)"
@@ -401,46 +468,97 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def flop_paths_summary(g, pot):
+    """Root strategy and EV read back through the query API (part of the
+    end-to-end step: what a caller of the solve reads)."""
+    q = g.query([])
+    return 4 * (q.strategy.size + q.ev.size + q.reach.size)
+
+
+def run_turn_secondary(args, grp, local):
+    """The turn workload's DCFR iterations/s (device-timed K captured-graph
+    iterations after W), reported inside the flop line."""
+    from poker_trainer_b200.solver import Solver
+
+    cfg = workload_config("turn", args.precision)
+    g = Solver.new(cfg)
+    g.iterate(args.warmup)
+    g.synchronize()
+    grp.barrier()
+    g.iterate(args.steps)
+    ms = grp.reduce(g.last_iterate_ms(), "max")
+    prof = g.iterate_profiled(args.steps)
+    kname, per_panel = g.terminal_kernel()
+    it_bytes = g.iteration_bytes()
+    g.close()
+    peak, peak_kind = measured_peak()
+    t = prof["classes"]["terminal"]
+    return {"workload": WORKLOADS["turn"], "value": grp.world * args.steps / (ms / 1000.0), "unit": UNIT,
+            "ms_per_iteration": ms / args.steps,
+            "iteration_roofline_frac": it_bytes * args.steps / (ms / 1000.0) / 1e9 / peak,
+            "terminal_kernel": f"{kname}_terminal_kernel", "terminals_per_panel": per_panel,
+            "terminal_gbs": t["bytes"] / (t["ms"] / 1000.0) / 1e9 if t["ms"] > 0 else None,
+            "terminal_frac": (t["bytes"] / (t["ms"] / 1000.0) / 1e9 / peak) if t["ms"] > 0 else None,
+            "peak_kind": f"of {peak_kind}"}
+
+
 def run_flop(args, world, rank, local):
-    """Time to 0.5%-of-pot exploitability on the flop workload: dcfr_solve from
-    a fresh solver with exploitability checks on the reference's schedule
-    (check every 10 iterations, then aimed at the predicted iteration), the
-    final exploitability re-checked by the FP64 best-response oracle; then K
-    profiled iterations for the roofline. The CPU figure is the oracle's
-    time per iteration on a bounded sample times the same iteration count
-    (the algorithm and its iteration count are the same on both sides), plus
-    one best-response pass per check."""
+    """Time to 0.5%-of-pot exploitability on the flop workload (the metric's
+    first term). The timed step is the whole solve: dcfr_solve from a fresh
+    solver, DCFR iterations with exploitability checks on the reference's
+    schedule (check every 10 iterations, then aimed at the predicted
+    iteration; lib.rs:158-172, 594-642), device-timed by CUDA events on the
+    solver's stream. The final exploitability is re-checked by the FP64
+    best-response oracle; K further profiled iterations give the per-class
+    breakdown and the terminal kernel's roofline. With N GPUs every rank
+    solves its own copy (replicas) and the job time is the maximum over
+    ranks."""
     import torch
+    from poker_trainer_b200.dist import Group
     from poker_trainer_b200.solver import Solver, SolveOptions
 
     torch.cuda.set_device(local)
+    grp = Group("nccl", torch.device("cuda", local), timeout_s=1200)
     cfg = workload_config("flop", args.precision)
     pot = float(cfg.root.pot)
-    t0 = time.perf_counter()
-    g = Solver.new(cfg)
-    t_create = time.perf_counter() - t0
+    # Warm-up: context, module load and clocks, on the turn workload (W
+    # iterations); the flop solver itself is created inside the timed e2e.
+    warm = Solver.new(workload_config("turn", args.precision))
+    warm.iterate(args.warmup)
+    warm.close()
     checks = []
     sampler = ClockSampler(local) if rank == 0 else None
     time.sleep(0.5)
+    grp.barrier()
     torch.cuda.synchronize()
+    # End to end: the host config in, dcfr_create, dcfr_solve to the target
+    # (each check reads one f64 back), the root's strategy and EVs read back.
+    t0 = time.perf_counter()
+    g = Solver.new(cfg)
+    t_create = time.perf_counter() - t0
     if sampler:
         sampler.begin()
     l0 = g.kernel_launches()
-    t0 = time.perf_counter()
     prog = g.solve(SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10),
                    on_progress=lambda pr: checks.append((pr.iteration, pr.exploitability_pct)) or True)
-    g.synchronize()
-    t_solve = time.perf_counter() - t0
     solve_launches = g.kernel_launches() - l0
     if sampler:
         sampler.end()
+    d2h_query = flop_paths_summary(g, pot)
+    g.synchronize()
+    t_e2e = time.perf_counter() - t0
+    solve_s = grp.reduce(g.last_solve_ms() / 1000.0, "max")
+    e2e_s = grp.reduce(t_e2e, "max")
     clocks = sampler.close() if sampler else None
+    setup = g.setup_profile()
     e32 = g.exploitability()
     e64, _ = g.exploitability_fp64()
     K = args.steps
     prof = g.iterate_profiled(K)
     it_bytes = g.iteration_bytes()
+    kname, per_panel = g.terminal_kernel()
     g.close()
+    turn = run_turn_secondary(args, grp, local) if not args.no_secondary else None
     ms = prof["total_ms"]
     peak, peak_kind = measured_peak()
     classes = prof["classes"]
@@ -452,79 +570,91 @@ def run_flop(args, world, rank, local):
     per_launch_ms = dc["ms"] / max(dc["launches"], 1)
     per_launch_bytes = dc["bytes"] / max(dc["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
-    kname = TERMINAL_KERNEL["flop"] if dom == "terminal" else KERNEL_NAMES[dom]
+    kfull = f"{kname}_terminal_kernel" if dom == "terminal" else KERNEL_NAMES[dom]
     cpu = None
-    if not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         steps, secs, used = time_oracle(cfg, threads, 1, args.cpu_flop_iters, None)
         per_it = secs / steps
         # A check is two best-response traversals: about one iteration.
         cpu_ttt = per_it * (prog.iteration + len(checks))
-        cpu = {"value": 1.0 / per_it, "unit": UNIT, "cores": used, "kind": "port",
+        cpu = {"value": cpu_ttt, "unit": "s", "cores": used, "kind": "port",
                "sample": f"{steps} DCFR iterations of the flop workload after 1 untimed, {secs:.1f} s on {used} host "
-                         f"threads (C++ restatement of the reference's CPU solver)",
-               "time_to_target_s": cpu_ttt,
-               "time_to_target_basis": f"{per_it:.3f} s/iteration x ({prog.iteration} iterations + "
-                                       f"{len(checks)} checks)"}
+                         f"threads (C++ restatement of the reference's CPU solver), scaled to the GPU solve's "
+                         f"{prog.iteration} iterations + {len(checks)} checks ({per_it:.3f} s per iteration); "
+                         f"bench.py --impl reference measures the full CPU solve",
+               "iters_per_s": 1.0 / per_it}
+    iters = prog.iteration
     line = {
-        "metric": METRIC, "value": K / (ms / 1000.0), "unit": UNIT, "n_gpus": world, "steps": K,
-        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": solve_s, "unit": "s", "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * solve_s / max(iters, 1), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOADS["flop"], "precision": args.precision, "storage": args.storage,
-                   "chance": chance_desc(), "parallelism": "single GPU",
-                   "l2": f"inputs larger than L2: one iteration moves {it_bytes / 1e9:.1f} GB"},
-        "time_to_target": {"seconds": t_solve, "iterations": prog.iteration, "checks": len(checks),
+                   "chance": chance_desc(),
+                   "parallelism": f"replicas x{world} (every rank solves the spot; job time is the max)"
+                                  if world > 1 else "single GPU",
+                   "step": "one DCFR iteration of the solve; value is the device time of the whole solve to 0.5% "
+                           "of the pot (its iterations and exploitability checks, CUDA events on the solver's "
+                           "stream), ms_per_step that time per iteration",
+                   "warmup": "W DCFR iterations of the turn workload before the timed solve (context, module, "
+                             "clocks)",
+                   "profiled": "K DCFR iterations after the solve, with events between kernel classes",
+                   "l2": f"inputs larger than L2: one iteration moves {it_bytes / 1e9:.1f} GB, no flush"},
+        "time_to_target": {"seconds": solve_s, "iterations": iters, "checks": len(checks),
                            "exploitability_pct": prog.exploitability_pct, "target_pct": 0.5,
-                           "create_seconds": t_create,
-                           "end_to_end_seconds": t_create + t_solve,
+                           "iters_per_s": iters / solve_s if solve_s > 0 else None,
                            "fp64_oracle_exploitability_pct": 100.0 * e64 / pot,
                            "f32_exploitability_pct": 100.0 * e32 / pot,
-                           "fp64_vs_f32_rel": abs(e64 - e32) / max(abs(e64), 1e-30),
-                           "speedup_vs_cpu": (cpu["time_to_target_s"] / t_solve) if cpu else None},
+                           "fp64_vs_f32_rel": abs(e64 - e32) / max(abs(e64), 1e-30)},
         "checks": checks,
         "clocks": clocks,
         "gpu_launches": int(solve_launches),
-        "e2e": {"value": prog.iteration / (t_create + t_solve), "unit": UNIT,
-                "h2d_bytes_per_step": C.sizeof(cfg) / max(prog.iteration, 1),
-                "d2h_bytes_per_step": 8.0 * len(checks) / max(prog.iteration, 1),
-                "what": "dcfr_create from the host config + dcfr_solve to the target with its exploitability "
-                        "checks (each reads one f64 back), wall clock; the iterations of the solve over that time"},
-        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": C.sizeof(cfg) / max(iters, 1),
+                "d2h_bytes_per_step": (8.0 * len(checks) + d2h_query) / max(iters, 1),
+                "create_seconds": t_create, "setup_ms": setup,
+                "what": "dcfr_create from the host config + dcfr_solve to the target (each check reads one f64 "
+                        "back) + the root's strategy and EVs read back, wall clock, max over ranks; bytes per "
+                        "iteration"},
+        "roofline": {"bound": "hbm", "kernel": kfull, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
-                     "traffic": ncu_traffic(kname, "flop"), "bytes_per_launch": per_launch_bytes,
-                     "ms_per_launch": per_launch_ms},
+                     "traffic": ncu_traffic(kfull, "flop"), "bytes_per_launch": per_launch_bytes,
+                     "ms_per_launch": per_launch_ms, "terminals_per_panel": per_panel},
         "iteration_roofline": {"bytes_per_iteration": it_bytes,
                                "achieved": it_bytes * (K / (ms / 1000.0)) / 1e9, "peak": peak, "unit": "GB/s",
                                "frac": it_bytes * (K / (ms / 1000.0)) / 1e9 / peak},
         "kernels": kernels,
+        "turn": turn,
         "cpu_baseline": cpu,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    grp.close()
     return 0
 
 
-def batch_configs(rank: int = 0):
-    """The 512 spots of one GPU; rank r of a multi-GPU run draws its own 512
-    (seed 3000 + 100003 r): independent units, weak scaling."""
+def batch_configs():
+    """The 512 spots of the batched workload (seed 3000). A multi-GPU run
+    partitions them across ranks (poker_trainer_b200.dist.shard)."""
     from poker_trainer_b200 import workloads
     from poker_trainer_b200.solver import Solver
 
     def nodes(c):
         st = Solver.estimate(c)
         return st.player_nodes + st.chance_nodes + st.terminal_nodes
-    return workloads.batched_river_spots(count=512, seed=3000 + 100003 * rank, estimate=nodes)
+    return workloads.batched_river_spots(count=512, seed=3000, estimate=nodes)
 
 
 def run_batch(args, world, rank, local):
-    """The batched river workload: every rank solves its own copy of the 512
-    spots (replicas); a step is one DCFR iteration of every spot, reported
-    as spot-iterations per second."""
+    """The batched river workload: the 512 spots are partitioned across the
+    ranks (each solves its contiguous share; strong scaling) and the
+    per-spot exploitabilities are gathered on rank 0; a step is one DCFR
+    iteration of every spot, reported as spot-iterations per second of the
+    whole job."""
     import numpy as np
     import torch
     from poker_trainer_b200.solver import BatchSolver
 
-    from poker_trainer_b200.dist import Group
+    from poker_trainer_b200.dist import Group, shard
 
     torch.cuda.set_device(local)
     grp = Group("nccl", torch.device("cuda", local))
@@ -532,7 +662,9 @@ def run_batch(args, world, rank, local):
     def reduce_max(x):
         return grp.reduce(x, "max")
 
-    cfgs = batch_configs(rank)
+    all_cfgs = batch_configs()
+    S_total = len(all_cfgs)
+    cfgs = shard(all_cfgs, rank, world)
     S = len(cfgs)
     K, W = args.steps, args.warmup
     # End to end: create from host configs, K iterations, storage of every spot read back.
@@ -574,7 +706,10 @@ def run_batch(args, world, rank, local):
     pots = np.array([c.root.pot for c in cfgs], np.float64)
     it_bytes = b.iteration_bytes()
     b.close()
-    value = world * S * K / (ms / 1000.0)
+    # Every spot's exploitability, gathered on rank 0 in spot order.
+    expl_all = np.asarray(grp.gather_concat(list(100.0 * np.asarray(expl) / pots)), np.float64)
+    it_bytes_all = grp.reduce(it_bytes, "sum")
+    value = S_total * K / (ms / 1000.0)
     peak, peak_kind = measured_peak()
     # The persistent kernel is the only kernel of the timed region: its
     # algorithmic bytes per launch are every spot's B_iter times the
@@ -612,24 +747,27 @@ def run_batch(args, world, rank, local):
                          f"over {threads} host threads (C++ restatement of the reference's CPU solver)"}
     line = {
         "metric": METRIC, "value": value, "unit": "spot-iterations/s", "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOADS["batch"], "spots": S, "iterations_per_step": 1,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "config": {"workload": WORKLOADS["batch"], "spots": S_total, "spots_per_rank": S, "iterations_per_step": 1,
+                   "parallelism": f"spots partitioned over {world} ranks" if world > 1 else "single GPU",
                    "tuning": {"warps": tuned.warps, "blocks_per_sm": tuned.blocks_per_sm,
                               "iterations_per_launch": tuned.iterations_per_launch,
                               "longest_first": tuned.longest_first, "candidates": tuned.candidates},
                    "l2": f"one iteration of all spots moves {it_bytes / 1e9:.2f} GB (> 126 MB L2), no flush"},
         "solve_ms": ms, "clocks": clocks,
-        "e2e": {"value": world * S * K / t_e2e, "unit": "spot-iterations/s",
+        "e2e": {"value": S_total * K / t_e2e, "unit": "spot-iterations/s",
                 "h2d_bytes_per_step": S * C.sizeof(cfgs[0]) / K, "d2h_bytes_per_step": d2h / K,
                 "what": "dcfr_batch_create + autotune + K iterations + every spot's storage read back, wall clock"},
         "gpu_launches": int(launches),
         "roofline": roof,
-        "iteration_roofline": {"bytes_per_iteration": it_bytes, "achieved": it_bytes * K / (ms / 1000.0) / 1e9,
-                               "peak": peak, "unit": "GB/s", "frac": it_bytes * K / (ms / 1000.0) / 1e9 / peak,
-                               "peak_kind": f"of {peak_kind}"},
-        "exploitability_pct_mean_after": float(np.mean(100.0 * expl / pots)),
+        "iteration_roofline": {"bytes_per_iteration": it_bytes_all,
+                               "achieved": it_bytes_all * K / (ms / 1000.0) / 1e9 / world,
+                               "peak": peak, "unit": "GB/s",
+                               "frac": it_bytes_all * K / (ms / 1000.0) / 1e9 / world / peak,
+                               "peak_kind": f"of {peak_kind} (per GPU)"},
+        "exploitability_pct_mean_after": float(np.mean(expl_all)) if rank == 0 else None,
+        "spots_gathered": int(len(expl_all)) if rank == 0 else None,
         "cpu_baseline": cpu,
     }
     if rank == 0:
@@ -763,7 +901,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=list(WORKLOADS), default="turn")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="flop")
     ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
     ap.add_argument("--storage", choices=["f32", "compressed"], default="f32",
                     help="turn, river, flop: f32 (the workloads' storage) or 16-bit compressed storage")
@@ -774,6 +912,7 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="flop: skip the turn workload's iters/s field")
     ap.add_argument("--max-iterations", type=int, default=2000, help="flop: iteration cap of the timed solve")
     ap.add_argument("--cpu-flop-iters", type=int, default=3, help="flop: oracle iterations timed for the CPU figure")
     ap.add_argument("--cpu-batch-iters", type=int, default=20, help="batch: oracle iterations per spot timed")
@@ -793,7 +932,11 @@ def main():
         if t < 1 or r < 1:
             ap.error("--sample deals at least one card per street")
         SAMPLE = (t, r, sd)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args.gpus)
     world, rank, local = dist_setup(args.gpus)
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; running {world} rank(s)", file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     if args.workload == "flop":

@@ -369,6 +369,35 @@ typedef struct dcfr_kernel_profile {
   double total_ms;                        /* first to last event */
 } dcfr_kernel_profile;
 
+/* Measurement hooks, no counterpart in the reference. dcfr_last_solve_ms:
+ * device time of the last dcfr_solve in milliseconds (CUDA events on the
+ * handle's stream at its start and end). dcfr_setup_profile: where the
+ * handle's setup went, host wall clock in milliseconds: the game (tree,
+ * hands, isomorphism) built on the host; device storage, hands and chance
+ * tables allocated and uploaded; strength tables and terminal layouts
+ * built on the device; both traversal plans built and uploaded; reach and
+ * value rows allocated; all of dcfr_create; and, when they happen, the
+ * iteration graph's capture (first dcfr_iterate / dcfr_solve) and the
+ * best-response and average graphs' (first exploitability or root values). */
+typedef struct dcfr_setup_profile {
+  double game_ms;
+  double device_ms;
+  double tables_ms;
+  double plans_ms;
+  double rows_ms;
+  double create_ms;
+  double iteration_graph_ms;
+  double eval_graphs_ms;
+} dcfr_setup_profile;
+int dcfr_last_solve_ms(const dcfr_solver* s, double* ms);
+int dcfr_setup_profile_get(const dcfr_solver* s, dcfr_setup_profile* out);
+
+/* Measurement hook, no counterpart in the reference: the terminal kernel
+ * this handle's f32 traversals launch (DCFR_TERMINAL_*), and for the panel
+ * kernel the terminals evaluated together per panel (0 otherwise). */
+enum { DCFR_TERMINAL_PANEL = 0, DCFR_TERMINAL_WARP = 1, DCFR_TERMINAL_BLOCK = 2, DCFR_TERMINAL_EXACT = 3 };
+int dcfr_terminal_kernel(const dcfr_solver* s, int32_t* kernel, int32_t* terminals_per_panel);
+
 /* Measurement hook, no counterpart in the reference: runs `iterations` DCFR
  * iterations (they advance the solve exactly as dcfr_iterate's) from a second
  * captured graph that also records a CUDA event on the handle's stream at
@@ -469,21 +498,25 @@ int dcfr_gemm_bf16_timed(const void* a, const void* b, void* c, int32_t m, int32
 
 /* No counterpart in the reference: range-vs-range showdown values on one
  * river board, for callers that cannot allocate device memory (a host whose
- * device memory belongs to its own pool allocator, or work enqueued while a
- * stream is being captured, where cudaMalloc is not allowed). It allocates
- * nothing: its scratch is one static device array of 192 KiB that every GPU
- * loading the library holds until exit. For each hero hand h,
+ * device memory belongs to its own pool allocator, or a process held to a
+ * fixed device-memory budget). It allocates nothing: its scratch is one
+ * static device array of 192 KiB that every GPU loading the library holds
+ * until exit. For each hero hand h,
  *   out[h] = win  * (sum of opp_reach over opponent hands weaker than h)
  *          + lose * (sum over stronger hands) + tie * (sum over equal hands),
  * counting only opponent hands that share no card with h (lose is signed:
  * pass a negative payoff). board (5 cards) and the two hand lists (2 card
  * ids per hand, no board cards, no repeats, at most DCFR_NOALLOC_MAX_HANDS
  * each) are host memory; opp_reach (n_opp floats) and out (n_hero floats)
- * are device memory; stream is a cudaStream_t (NULL: the default stream) and
- * the call is asynchronous on it. Calls share the scratch array: calls whose
- * work overlaps on the GPU race and must be serialised by the caller. The
- * first call on each device does a one-time set-up with that device current;
- * make it before any stream capture. */
+ * are device memory; opp_reach entries must be finite and >= 0 (a call
+ * given a negative, NaN or infinite entry writes NaN to every out entry).
+ * stream is a cudaStream_t (NULL: the default stream) and the call is
+ * asynchronous on it. Calls share the scratch array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller. The first
+ * call on each device does a one-time set-up with that device current and
+ * caches it for the process (resetting the device while the library is
+ * loaded is not supported); make that first call before any stream
+ * capture. */
 int dcfr_showdown_values_noalloc(const uint8_t board[5], const uint8_t* hero_cards, int32_t n_hero,
                                  const uint8_t* opp_cards, int32_t n_opp, const float* opp_reach, double win,
                                  double lose, double tie, float* out, void* stream);

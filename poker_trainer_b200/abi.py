@@ -133,6 +133,12 @@ class KernelProfile(C.Structure):
     ]
 
 
+class SetupProfile(C.Structure):
+    """dcfr_setup_profile (include/dcfr.h): host milliseconds per setup phase."""
+    _fields_ = [(n, C.c_double) for n in ("game_ms", "device_ms", "tables_ms", "plans_ms", "rows_ms", "create_ms",
+                                          "iteration_graph_ms", "eval_graphs_ms")]
+
+
 class BatchTuning(C.Structure):
     """dcfr_batch_tuning (include/dcfr.h)."""
     _fields_ = [

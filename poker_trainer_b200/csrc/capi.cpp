@@ -417,6 +417,27 @@ int dcfr_iteration_bytes(const dcfr_solver* s, double* bytes) {
   return DCFR_OK;
 }
 
+int dcfr_last_solve_ms(const dcfr_solver* s, double* ms) {
+  NEED(s);
+  if (!ms) return fail(DCFR_ERR_INVALID_ARG, "NULL out");
+  *ms = s->e->last_solve_ms;
+  return DCFR_OK;
+}
+
+int dcfr_setup_profile_get(const dcfr_solver* s, dcfr_setup_profile* out) {
+  NEED(s);
+  if (!out) return fail(DCFR_ERR_INVALID_ARG, "NULL out");
+  *out = s->e->setup;
+  return DCFR_OK;
+}
+
+int dcfr_terminal_kernel(const dcfr_solver* s, int32_t* kernel, int32_t* terminals_per_panel) {
+  NEED(s);
+  if (!kernel || !terminals_per_panel) return fail(DCFR_ERR_INVALID_ARG, "NULL out");
+  s->e->terminal_kernel(*kernel, *terminals_per_panel);
+  return DCFR_OK;
+}
+
 int dcfr_iterate_profiled(dcfr_solver* s, uint32_t iterations, dcfr_kernel_profile* out) {
   NEED(s);
   if (!out) return fail(DCFR_ERR_INVALID_ARG, "out is NULL");

@@ -4,7 +4,9 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <unordered_map>
@@ -54,6 +56,7 @@ Plan::~Plan() {
   dfree(d_tasks);
   dfree(d_fast);
   dfree(d_units);
+  dfree(d_panels);
   dfree(d_leaves);
   dfree(d_trees);
   dfree(d_fdown);
@@ -101,7 +104,13 @@ static uint32_t next_gap(bool has_prev, uint32_t t0, double e0, uint32_t t, doub
   return std::min(std::max(gu, min_gap), max_gap);
 }
 
+// Milliseconds since t0 (host clock), for the setup profile.
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 Status Engine::create(const dcfr_config& cfg, std::unique_ptr<Engine>& out) {
+  const auto t0 = std::chrono::steady_clock::now();
   std::unique_ptr<Engine> e(new Engine());
   Status s;
   if (cfg.precision != DCFR_PRECISION_FAST && cfg.precision != DCFR_PRECISION_EXACT) {
@@ -112,8 +121,10 @@ Status Engine::create(const dcfr_config& cfg, std::unique_ptr<Engine>& out) {
   e->fast_ = cfg.precision == DCFR_PRECISION_FAST;
   s.code = build_game(cfg, e->g, s.msg, true);
   if (!s.ok()) return s;
+  e->setup.game_ms = ms_since(t0);
   s = e->init();
   if (!s.ok()) return s;
+  e->setup.create_ms = ms_since(t0);
   out = std::move(e);
   return Status();
 }
@@ -227,6 +238,11 @@ double Engine::iteration_bytes() const {
 }
 
 Status Engine::init() {
+  auto t0 = std::chrono::steady_clock::now();
+  auto phase = [&](double& slot) {
+    slot += ms_since(t0);
+    t0 = std::chrono::steady_clock::now();
+  };
   last_exploitability = INFINITY;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CK(cudaEventCreate(&ev0_));
@@ -325,6 +341,7 @@ Status Engine::init() {
     if (!(s = dalloc(iso_, iso.size(), "iso refs")).ok()) return s;
     if (!iso.empty()) CK(cudaMemcpy(iso_, iso.data(), iso.size() * sizeof(IsoRefD), cudaMemcpyHostToDevice));
   }
+  phase(setup.device_ms);
   // Strength tables, built on the device.
   {
     const int nb = (int)g.boards.size();
@@ -353,12 +370,14 @@ Status Engine::init() {
     }
     if (fast_ && !(s = ensure_fast_layouts()).ok()) return s;
   }
+  phase(setup.tables_ms);
   // Plans for the two traversals of an iteration.
   for (int p = 0; p < 2; p++) {
     full_[p].reset(new Plan());
     if (!(s = build_plan(0, p, *full_[p])).ok()) return s;
     max_slots_ = std::max<uint64_t>(max_slots_, full_[p]->nslots);
   }
+  phase(setup.plans_ms);
   // Rows.
   if (!(s = dalloc(reach_, (size_t)max_slots_ * stride_, "reach rows")).ok()) return s;
   if (!(s = dalloc(vals_, (size_t)N * stride_, "value rows")).ok()) return s;
@@ -373,6 +392,7 @@ Status Engine::init() {
     CK(cudaMemcpy(root_rows_, rr.data(), rr.size() * 4, cudaMemcpyHostToDevice));
     if (!(s = dalloc(root_out_, rr.size(), "root rows")).ok()) return s;
   }
+  phase(setup.rows_ms);
   // Terminal scratch, sized for the largest terminal launch of the two plans.
   if (!fast_) {
     for (int p = 0; p < 2; p++)
@@ -390,6 +410,7 @@ Status Engine::init() {
   }
   for (int p = 0; p < 2; p++)
     if (!(s = upload_plan(*full_[p])).ok()) return s;
+  phase(setup.plans_ms);
   if (!(s = dalloc(cur_disc_, 1, "discounts")).ok()) return s;
   if (!(s = dalloc(counter_, 1, "counter")).ok()) return s;
   CK(cudaMemsetAsync(counter_, 0, 4, stream_));
@@ -425,6 +446,31 @@ Status Engine::ensure_fast_layouts() {
     return s;
   }
   fast_blocks_ = sms * per_sm;
+  // The f32 solve's terminal kernel: panels of 8 terminals where that
+  // layout fits a block, else panels of 4; DCFR_TERMINAL_KERNEL selects
+  // another one (panel, panel4, panel8, warp, block) for comparisons.
+  const char* sel = std::getenv("DCFR_TERMINAL_KERNEL");
+  const std::string want = sel ? sel : "panel";
+  term_kernel_ = want == "warp" ? TK_WARP : want == "block" ? TK_BLOCK : TK_PANEL;
+  if (term_kernel_ == TK_PANEL) {
+    const int o0 = 1, o1 = 0;  // opponent of traverser 0 and 1
+    panel_T_ = panel_E_ = panel_blocks_ = 0;
+    for (int T : {8, 4}) {
+      if ((want == "panel4" && T != 4) || (want == "panel8" && T != 8)) continue;
+      // One setup per traverser: the shared-memory footprint depends on both
+      // players' padded hand counts; the larger one sets the limit.
+      int b0 = 0, b1 = 0;
+      const int e0 = panel_terminal_setup(hp_[o0], hp_[0], fcstride_, tstride_, T, b0);
+      const int e1 = panel_terminal_setup(hp_[o1], hp_[1], fcstride_, tstride_, T, b1);
+      if (e0 > 0 && e1 > 0 && e0 == e1) {
+        panel_T_ = T;
+        panel_E_ = e0;
+        panel_blocks_ = sms * std::min(b0, b1);
+        break;
+      }
+    }
+    if (panel_T_ == 0) term_kernel_ = tstride_ <= WARP_TERMINAL_MAX_HANDS ? TK_WARP : TK_BLOCK;
+  }
   for (int k = 0; k < 2; k++) {
     int bps = 0;
     term_warps_[k] = warp_terminal_setup(stride_, fcstride_, tstride_, k ? 8 : 4, 16, bps);
@@ -781,15 +827,25 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       by_fold[layout].push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, layout, L.slot, L.row,
                                          NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
     }
+  // Within a layout, showdowns and folds are interleaved evenly in chunks of
+  // PT tasks (after k chunks, about k |S| / (|S| + |F|) showdown chunks).
+  // With the panel kernel a chunk is a panel, all showdowns or all folds.
   plan.h_fast.clear();
+  plan.h_panels.clear();
+  const bool panels = fast_ && term_kernel_ == TK_PANEL;
+  const size_t PT = panels ? (size_t)panel_T_ : 1;
   for (uint32_t l = 0; l <= nb; l++) {
     const std::vector<FastTask>& S = by_sd[l];
     const std::vector<FastTask>& F = by_fold[l];
-    // Interleave evenly: after k tasks, about k * |S| / (|S| + |F|) showdowns.
+    const size_t ns = (S.size() + PT - 1) / PT, nf = (F.size() + PT - 1) / PT;
     size_t i = 0, j = 0;
-    while (i < S.size() || j < F.size()) {
-      if (j >= F.size() || (i < S.size() && i * F.size() <= j * S.size())) plan.h_fast.push_back(S[i++]);
-      else plan.h_fast.push_back(F[j++]);
+    while (i < ns || j < nf) {
+      const bool take_s = j >= nf || (i < ns && i * nf <= j * ns);
+      const std::vector<FastTask>& V = take_s ? S : F;
+      const size_t c = take_s ? i++ : j++;
+      const size_t a = c * PT, e = std::min(V.size(), a + PT);
+      if (panels) plan.h_panels.push_back(PanelD{(uint32_t)plan.h_fast.size(), (uint32_t)(e - a), l, 0});
+      plan.h_fast.insert(plan.h_fast.end(), V.begin() + a, V.begin() + e);
     }
   }
   // Units of the warp terminal kernel: maximal runs of tasks on one layout
@@ -894,6 +950,10 @@ Status Engine::upload_plan(Plan& plan) {
                   cudaMemcpyHostToDevice));
   if (!plan.h_units.empty())
     CK(cudaMemcpy(plan.d_units, plan.h_units.data(), plan.h_units.size() * sizeof(TermUnit), cudaMemcpyHostToDevice));
+  if (!(s = dalloc(plan.d_panels, plan.h_panels.size(), "plan")).ok()) return s;
+  if (!plan.h_panels.empty())
+    CK(cudaMemcpy(plan.d_panels, plan.h_panels.data(), plan.h_panels.size() * sizeof(PanelD),
+                  cudaMemcpyHostToDevice));
   if (!(s = dalloc(plan.d_trees, plan.h_trees.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fdown, plan.h_fdown.size(), "plan")).ok()) return s;
   if (!(s = dalloc(plan.d_fup, plan.h_fup.size(), "plan")).ok()) return s;
@@ -1025,9 +1085,13 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
     if (!plan.h_fast.empty()) {
       FastArgs F;
       fast_args(p, F);
-      // Warp per terminal for short rows; one block-wide scan per terminal
-      // for long rows, where a warp alone would scan too many elements.
-      if (tstride_ <= WARP_TERMINAL_MAX_HANDS)
+      // Panels of T terminals per block; or (a selectable alternative) a
+      // warp per terminal for short rows and one block-wide scan per
+      // terminal for long rows.
+      if (term_kernel_ == TK_PANEL)
+        launch_panel_terminal(F, plan.d_fast, plan.d_panels, (int)plan.h_panels.size(), panel_T_, panel_E_,
+                              panel_blocks_, stream_);
+      else if (term_kernel_ == TK_WARP)
         launch_warp_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
                              term_warps_[0], term_blocks_[0],
                              stream_);
@@ -1198,6 +1262,7 @@ Status Engine::ensure_discounts(uint32_t max_t) {
 
 Status Engine::capture_graphs() {
   if (iter_graph_) return Status();
+  const auto t0 = std::chrono::steady_clock::now();
   cudaGraph_t graph;
   // One DCFR iteration: t += 1, then player 0's and player 1's traversals
   // with the same discounts (lib.rs:577-585).
@@ -1209,6 +1274,16 @@ Status Engine::capture_graphs() {
   CK(cudaGraphInstantiate(&iter_graph_, graph, 0));
   cudaGraphDestroy(graph);
   iter_kernels_ = 1 + full_[0]->kernels + full_[1]->kernels;
+  setup.iteration_graph_ms += ms_since(t0);
+  return Status();
+}
+
+// The best-response and average-strategy traversal pairs (exploitability,
+// root values), captured on their first use.
+Status Engine::capture_eval_graphs() {
+  if (br_graph_) return Status();
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaGraph_t graph;
   for (int mode : {M_BR, M_AVG}) {
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     enqueue_traversal(*full_[0], mode, root_rows_, root_out_);
@@ -1218,6 +1293,7 @@ Status Engine::capture_graphs() {
     cudaGraphDestroy(graph);
   }
   pair_kernels_ = full_[0]->kernels + full_[1]->kernels;
+  setup.eval_graphs_ms += ms_since(t0);
   return Status();
 }
 
@@ -1331,7 +1407,7 @@ Status Engine::sync() {
 // root_values (cfr.rs:482-490): sum over hands of value * weight in f64.
 Status Engine::mode_root_values(int mode, double out[2]) {
   Status s;
-  if (!(s = capture_graphs()).ok()) return s;
+  if (!(s = capture_eval_graphs()).ok()) return s;
   CK(cudaGraphLaunch(mode == M_BR ? br_graph_ : avg_graph_, stream_));
   launches += pair_kernels_;
   std::vector<float> rows((size_t)2 * stride_);
@@ -1492,8 +1568,24 @@ Status Engine::traverse(int p, int mode, uint32_t t, float* out) {
   return Status();
 }
 
+// dcfr_solve with its device time: CUDA events on the handle's stream at
+// the start and at the end (iterations, checks and any first-use graph
+// capture between them).
 Status Engine::solve(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb, void* user,
                      dcfr_progress& progress) {
+  CK(cudaEventRecord(ev0_, stream_));
+  Status s = solve_loop(opts, cancel, cb, user, progress);
+  if (!s.ok()) return s;
+  CK(cudaEventRecord(ev1_, stream_));
+  CK(cudaEventSynchronize(ev1_));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  last_solve_ms = ms;
+  return Status();
+}
+
+Status Engine::solve_loop(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb,
+                          void* user, dcfr_progress& progress) {
   const double pot = (double)g.cfg.root.pot;
   const uint32_t check_every = std::max(opts.check_every, 1u);
   progress.iteration = iterations;

@@ -49,6 +49,9 @@ void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const Te
                             int warps,
                             int max_blocks, cudaStream_t s);
 int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
+int panel_terminal_setup(int hpo, int hpp, int cstride, int tstride, int T, int& blocks_per_sm);
+void launch_panel_terminal(const FastArgs& A, const FastTask* tasks, const PanelD* panels, int npanels, int T, int e,
+                           int max_blocks, cudaStream_t s);
 // FP64 best-response oracle kernels (br64.cu).
 void launch_down64(const Row64Args& A, const DownTask* tasks, int ntasks, int hp, cudaStream_t s);
 void launch_up64(int mode, const Row64Args& A, const UpTask* tasks, int ntasks, int hp, cudaStream_t s);
@@ -89,6 +92,8 @@ struct Plan {
   std::vector<FastTask> h_fast;  // fast precision: one task per terminal
   std::vector<TermUnit> h_units; // runs of h_fast on one layout (warp terminal kernel)
   TermUnit* d_units = nullptr;
+  std::vector<PanelD> h_panels;  // panels of h_fast (panel terminal kernel)
+  PanelD* d_panels = nullptr;
   std::vector<LeafTask> h_leaves; // depth-limited solves: the leaves of this traversal
   LeafTask* d_leaves = nullptr;
   // Fused river subtrees (one block each) and their tasks.
@@ -161,6 +166,8 @@ class Engine {
   double last_exploitability;
   uint64_t launches = 0;
   double last_iterate_ms = 0.0;
+  double last_solve_ms = 0.0;
+  dcfr_setup_profile setup{};
 
   Status iterate(uint32_t n);
   Status iterate_profiled(uint32_t n, dcfr_kernel_profile& out);
@@ -188,6 +195,11 @@ class Engine {
   Status ranges_after(const std::vector<dcfr_step>& path, float out[2][DCFR_NUM_COMBOS]);
   Status actions_at(const std::vector<dcfr_step>& path, std::vector<Act>& out, bool& decision);
   double iteration_bytes() const;
+  // The f32 traversals' terminal kernel (DCFR_TERMINAL_*) and panel width.
+  void terminal_kernel(int32_t& kernel, int32_t& per_panel) const {
+    kernel = fast_ ? term_kernel_ : DCFR_TERMINAL_EXACT;
+    per_panel = fast_ && term_kernel_ == TK_PANEL ? panel_T_ : 0;
+  }
   int isomorphic_pairs() const;
   // Offset of a decision node's block in the reference storage layout.
   Status node_storage(const std::vector<dcfr_step>& path, uint64_t& offset, int& num_actions, int& num_hands);
@@ -245,6 +257,11 @@ class Engine {
   int fcstride_ = 0, femax_ = 0, fast_blocks_ = 0;
   // Warp terminal kernel: warps per block and blocks (float rows, double rows).
   int term_warps_[2] = {0, 0}, term_blocks_[2] = {0, 0};
+  // Terminal kernel of the f32 solve in fast precision, and the panel
+  // kernel's terminals per panel, elements per thread and blocks.
+  enum TermKernel { TK_PANEL = DCFR_TERMINAL_PANEL, TK_WARP = DCFR_TERMINAL_WARP, TK_BLOCK = DCFR_TERMINAL_BLOCK };
+  int term_kernel_ = TK_PANEL;
+  int panel_T_ = 0, panel_E_ = 0, panel_blocks_ = 0;
   // Depth-limited solves: the leaf-value network and its buffers.
   dcfr_mlp* net_ = nullptr;
   float* leaf_reach_[2] = {nullptr, nullptr};
@@ -294,6 +311,9 @@ class Engine {
   void enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out);
   Status ensure_discounts(uint32_t max_t);
   Status capture_graphs();
+  Status capture_eval_graphs();
+  Status solve_loop(const dcfr_solve_options& opts, const volatile int32_t* cancel, dcfr_progress_cb cb, void* user,
+                    dcfr_progress& progress);
   void free_graphs();
   Status mode_root_values(int mode, double out[2]);
   Status walk(const std::vector<dcfr_step>& path, uint32_t& node, std::vector<float> reach[2],

@@ -5,10 +5,10 @@
 //
 // Who needs it: callers that must not call cudaMalloc/cudaFree. Examples are
 // a host whose device memory is owned by its own pool allocator (a trainer
-// sharing the GPU with a framework's caching allocator), code that enqueues
-// work while a stream is being captured (allocation calls are not allowed in
-// a capture), and latency-sensitive loops where an allocation's implicit
-// device synchronisation would stall other streams.
+// sharing the GPU with a framework's caching allocator that has reserved
+// the device), a process held to a fixed device-memory budget, and
+// latency-sensitive loops where an allocation's implicit device
+// synchronisation would stall other streams.
 //
 // Limits and sharing rules:
 // - at most DCFR_NOALLOC_MAX_HANDS (1326) hands per side; larger sizes are
@@ -22,6 +22,11 @@
 // - the first call on each device does a one-time set-up with that device
 //   current (resolving the array's device address and the terminal kernel's
 //   shared-memory limit); make that first call before any stream capture.
+//   The set-up is cached for the life of the process: resetting the device
+//   (cudaDeviceReset) while the library is loaded is not supported;
+// - opp_reach must be finite and >= 0 (reach probabilities times weights):
+//   the exact fixed-point sums assume it. A call given a negative, NaN or
+//   infinite entry writes NaN to every out entry instead of values.
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -94,8 +99,14 @@ __global__ void __launch_bounds__(1024) noalloc_prep_kernel(Scratch* S, const __
       S->hc1[q][h] = in ? P.cards[q][2 * h] : 255;
       S->hc2[q][h] = in ? P.cards[q][2 * h + 1] : 255;
     }
-  for (int h = tid; h < NA_HP; h += blockDim.x) S->reach[h] = h < P.n[1] ? reach[h] : 0.0f;
-  __syncthreads();
+  // Entries that are negative, NaN or infinite: the call's output is NaN.
+  int bad = 0;
+  for (int h = tid; h < NA_HP; h += blockDim.x) {
+    const float r = h < P.n[1] ? reach[h] : 0.0f;
+    bad |= !(r >= 0.0f && r <= 3.402823466e38f);
+    S->reach[h] = r;
+  }
+  bad = __syncthreads_or(bad);
   for (int j = tid; j < P.n[1]; j += blockDim.x) {
     const int a = P.cards[1][2 * j], b = P.cards[1][2 * j + 1];
     const int hi = a > b ? a : b, lo = a > b ? b : a;
@@ -112,8 +123,12 @@ __global__ void __launch_bounds__(1024) noalloc_prep_kernel(Scratch* S, const __
     }
     S->same[h] = sm;
   }
+  // A rejected row leaves the task dead (the terminal kernel skips it) and
+  // the values NaN.
+  if (bad)
+    for (int h = tid; h < NA_HP; h += blockDim.x) S->vals[h] = __int_as_float(0x7fc00000);
   if (tid == 0) {
-    S->alive[0] = 1;
+    S->alive[0] = bad ? 0 : 1;
     S->alive[1] = 0;
     FastTask t;
     t.kind = T_SHOWDOWN_BATCH;
@@ -231,6 +246,9 @@ extern "C" int dcfr_showdown_values_noalloc(const uint8_t board[5], const uint8_
   uint16_t* seg = AT(uint16_t, seg);
   uint4* rec = AT(uint4, rec);
 
+  // Launch errors below are this call's: clear any left by earlier work on
+  // this thread.
+  (void)cudaGetLastError();
   noalloc_prep_kernel<<<1, 1024, 0, s>>>(S, P, opp_reach);
   launch_strength(AT(uint8_t, board), 1, hc1_0, hc2_0, hc1_1, hc2_1, n_hero, n_opp, tables, count, NA_HP, s);
   launch_fast_layouts(tables, count, NA_HP, 1, hc1_0, hc2_0, hc1_1, hc2_1, n_hero, n_opp, cat, seg, rec, NA_CSTRIDE,

@@ -153,6 +153,16 @@ struct TermUnit {
   uint32_t pad;
 };
 
+// A panel of the panel terminal kernel (terminal_panel.cu): `count` (1..T)
+// consecutive fast terminal tasks, all on one layout and all showdowns or
+// all folds.
+struct PanelD {
+  uint32_t first;   // first task
+  uint32_t count;   // tasks
+  uint32_t layout;  // FastTask::board of every task in the panel
+  uint32_t pad;
+};
+
 // Per (layout, traverser) scan layout of the opponent's hands: segment 0
 // lists them in ascending strength, segment 1+c lists those holding card c
 // (ascending strength). seg[j] is the first element of segment j

@@ -1,0 +1,351 @@
+// Panel terminal evaluation: the fast-precision terminal kernel of the solve
+// (f32 rows).
+//
+// It computes what fast_terminal_kernel and warp_terminal_kernel compute
+// (terminal_fast.cu, warp_terminal.cuh): every fold and showdown value of
+// the reference's evaluators (crates/solver/src/eval.rs:40-379) from exact
+// 64-bit fixed-point prefix sums over a board's scan layout, with the same
+// integer sums and the same final f64/f32 operations, so its results are
+// bit-identical to theirs.
+//
+// What changes is the shape of the work. A panel is up to T terminals of
+// one layout (one river board, or the fold layout). A block evaluates a
+// panel's T terminals together:
+//   - the T reach rows are staged row-major with a padded stride, so the T
+//     lanes that gather one layout element read T different banks;
+//   - the prefix array is interleaved [element][T]: lane t of a group of T
+//     lanes works on terminal t, and the T lanes that look up one position
+//     read T consecutive 8-byte prefixes instead of T scattered ones;
+//   - the layout (elements, per-hand records, segment starts) and every
+//     per-hand record read is shared by the T terminals.
+// A random 8-byte gather by 32 lanes costs several shared-memory wavefronts
+// (bank conflicts); 32/T random gathers of T x 8 contiguous bytes cost
+// close to the minimum. The scan keeps each thread's E layout elements in
+// registers between its two passes, so the prefix array is written once.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.hpp"
+#include "warp_terminal.cuh"
+
+namespace dcfr {
+
+constexpr int PANEL_THREADS = 512;
+constexpr int PANEL_WARPS = PANEL_THREADS / 32;
+
+// Shared-memory layout of a block (every offset 16-byte aligned).
+struct PanelSmem {
+  size_t rows, g, cat, rec, same, seg, cs, wsum, wmax, total;
+  int rstride;  // floats per staged row: hpo + 4 (16-byte rows; bank stagger)
+  __host__ __device__ PanelSmem(int hpo, int hpp, int cstride, int tstride, int T) {
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    rstride = hpo + 4;
+    rows = 0;                                                  // [2][T][rstride] f32
+    g = up16(rows + (size_t)2 * T * rstride * 4);              // [cstride + 1][T] i64
+    cat = up16(g + ((size_t)cstride + 1) * T * 8);             // [cstride] u16
+    rec = up16(cat + (size_t)cstride * 2);                     // [tstride] uint4
+    same = up16(rec + (size_t)tstride * 16);                   // [hpp] u16
+    seg = up16(same + (size_t)hpp * 2);                        // [FAST_SEGS] u16
+    cs = up16(seg + FAST_SEGS * 2);                            // [52][T] {start prefix, total}
+    wsum = up16(cs + (size_t)52 * T * 16);                     // [PANEL_WARPS][T] i64
+    wmax = up16(wsum + (size_t)PANEL_WARPS * T * 8);           // [PANEL_WARPS] f32
+    total = up16(wmax + (size_t)PANEL_WARPS * 4);
+  }
+};
+
+__device__ __forceinline__ void panel_cp16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// One block per SM. Block b takes the contiguous panel range
+// [b N / G, (b+1) N / G) (panels are ordered by layout) and stages a
+// layout when its range enters it. Per panel, five block barriers:
+//   (A) the panel's rows have landed (cp.async) and the previous panel is done;
+//   (B) per-warp row maxima written (and a new layout staged);
+//   (C) per-warp scan totals written;
+//   (D) prefixes written;
+//   (E) per-card segment starts and totals written.
+// The next panel's rows are copied in (cp.async) while this one runs.
+template <int T, int E>
+__global__ void __launch_bounds__(PANEL_THREADS, 1)
+    panel_terminal_kernel(FastArgs A, const FastTask* __restrict__ tasks, const PanelD* __restrict__ panels,
+                          int npanels) {
+  extern __shared__ __align__(16) unsigned char smem_panel[];
+  const int p = A.p, o = p ^ 1;
+  const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
+  const PanelSmem Ls(hpo, hpp, A.cstride, A.tstride, T);
+  float* rows = reinterpret_cast<float*>(smem_panel + Ls.rows);
+  long long* G = reinterpret_cast<long long*>(smem_panel + Ls.g);
+  uint16_t* scat = reinterpret_cast<uint16_t*>(smem_panel + Ls.cat);
+  uint4* srec = reinterpret_cast<uint4*>(smem_panel + Ls.rec);
+  uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_panel + Ls.same);
+  uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_panel + Ls.seg);
+  longlong2* cs = reinterpret_cast<longlong2*>(smem_panel + Ls.cs);
+  long long* wsum = reinterpret_cast<long long*>(smem_panel + Ls.wsum);
+  float* wmax = reinterpret_cast<float*>(smem_panel + Ls.wmax);
+  const int rstride = Ls.rstride;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t = lane % T;                          // this thread's terminal within a panel
+  constexpr int CPW = 32 / T;                      // scan chunks per warp
+  const int k0 = (warp * CPW + lane / T) * E;      // first layout element of this thread's chunk
+  constexpr int HSTEP = PANEL_THREADS / T;         // hands per value pass
+
+  const int b0 = (int)(((long long)blockIdx.x * npanels) / gridDim.x);
+  const int b1 = (int)(((long long)(blockIdx.x + 1) * npanels) / gridDim.x);
+  if (b0 >= b1) return;
+
+  for (int h = tid; h < hpp; h += PANEL_THREADS) {
+    const uint32_t sm = h < np ? A.same[h] : NONE32;
+    ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
+  }
+  // Rows of panel pi into buffer b: T x (hpo / 4) 16-byte copies; rows of
+  // dead subtrees (and missing tasks) are not copied.
+  auto prefetch = [&](int pi, int b) {
+    const PanelD P = panels[pi];
+    const int per = hpo >> 2;
+    float* dst = rows + (size_t)b * T * rstride;
+    for (int i = tid; i < (int)P.count * per; i += PANEL_THREADS) {
+      const int tt = i / per, j = i - tt * per;
+      const uint32_t slot = tasks[P.first + tt].slot;
+      if (A.alive[slot] != 0)
+        panel_cp16(dst + (size_t)tt * rstride + 4 * j, A.reach + (size_t)slot * A.stride + 4 * j);
+    }
+    cp_async_commit();
+  };
+  prefetch(b0, 0);
+  uint32_t layout = NONE32;
+  int L = 0;
+
+  for (int pi = b0; pi < b1; pi++) {
+    const int buf = (pi - b0) & 1;
+    cp_async_wait<0>();
+    __syncthreads();  // (A)
+    if (pi + 1 < b1) prefetch(pi + 1, buf ^ 1);
+    const PanelD P = panels[pi];
+    const float* rbase = rows + (size_t)buf * T * rstride;
+    // Row maxima: warp w reduces part w / T of row w % T.
+    {
+      const int tt = warp % T, part = warp / T;
+      constexpr int PARTS = PANEL_WARPS / T;
+      const float4* r4 = reinterpret_cast<const float4*>(rbase + (size_t)tt * rstride);
+      float mx = 0.0f;
+      for (int i = part * 32 + lane; i < (hpo >> 2); i += 32 * PARTS) {
+        const float4 v = r4[i];
+        mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+      if (lane == 0) wmax[warp] = mx;
+    }
+    if (P.layout != layout) {
+      layout = P.layout;
+      const size_t lay = (size_t)layout * 2 + p;
+      const uint16_t* gseg = A.seg + lay * FAST_SEGS;
+      if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
+      const int Ln = gseg[FAST_SEGS - 1];
+      const uint16_t* gcat = A.cat + lay * A.cstride;
+      for (int k = tid; k < Ln; k += PANEL_THREADS) scat[k] = gcat[k];
+      const uint4* grec = A.rec + lay * A.tstride;
+      for (int h = tid; h < np; h += PANEL_THREADS) srec[h] = grec[h];
+    }
+    __syncthreads();  // (B)
+    L = sseg[FAST_SEGS - 1];
+    // This thread's task (lane t of the panel).
+    const bool has = t < (int)P.count;
+    const FastTask tk = tasks[P.first + (has ? t : 0)];
+    const bool live = has && A.alive[tk.slot] != 0;
+    float mx = 0.0f;
+#pragma unroll
+    for (int w = t; w < PANEL_WARPS; w += T) mx = fmaxf(mx, wmax[w]);
+    const int S = scale_exponent(mx);
+    const double scale = pow2(S), inv = pow2(-S);
+    const float* myrow = rbase + (size_t)t * rstride;
+
+    // Scan: E consecutive elements per thread, held in registers.
+    long long x[E];
+    long long local = 0;
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+      const int k = k0 + i;
+      long long v = 0;
+      if (live && k < L) v = fixed(myrow[scat[k]], scale);
+      x[i] = v;
+      local += v;
+    }
+    long long inc = local;
+#pragma unroll
+    for (int d = T; d < 32; d <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= d) inc += y;
+    }
+    if (lane >= 32 - T) wsum[warp * T + t] = inc;
+    __syncthreads();  // (C)
+    long long acc = inc - local;
+    for (int w = 0; w < warp; w++) acc += wsum[w * T + t];
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+      const int k = k0 + i;
+      if (k <= L) G[(size_t)k * T + t] = acc;
+      acc += x[i];
+    }
+    __syncthreads();  // (D)
+    for (int i = tid; i < 52 * T; i += PANEL_THREADS) {
+      const int c = i / T, tt = i - c * T;
+      const long long s0 = G[(size_t)sseg[1 + c] * T + tt];
+      cs[i] = make_longlong2(s0, G[(size_t)sseg[2 + c] * T + tt] - s0);
+    }
+    __syncthreads();  // (E)
+
+    if (!live) continue;  // dead subtree (cfr.rs:267-274) or no task: rows untouched
+    const uint32_t kind = tk.kind;
+    const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
+    const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
+    const double pa = tk.a * inv, pb = tk.b * inv, pc = tk.c * inv, pd = tk.d * inv;
+    const long long T0 = G[(size_t)sseg[1] * T + t];
+    float* out = A.vals + (size_t)tk.row * A.stride;
+    float* fout = tk.frow != NONE32 ? A.vals + (size_t)tk.frow * A.stride : nullptr;
+    auto value = [&](int h, float& v, float& fv) {
+      v = 0.0f;
+      fv = 0.0f;
+      if (h >= np) return;
+      const uint4 q = srec[h];
+      const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
+      const longlong2 ca = cs[a * T + t], cb = cs[b * T + t];
+      const uint16_t sm = ssame[h];
+      const long long si = sm == 0xFFFF ? 0ll : fixed(myrow[sm], scale);
+      const long long F = T0 - ca.y - cb.y + si;
+      if (fold) {
+        // eval_fold (eval.rs:40-64) returns zeros on a zero total.
+        v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
+        return;
+      }
+      if (q.w >> 16) {
+        const long long Gw = G[(size_t)(q.x & 0xFFFF) * T + t], Gs = G[(size_t)(q.x >> 16) * T + t];
+        const long long Gaw = G[(size_t)(q.y & 0xFFFF) * T + t], Gas = G[(size_t)(q.y >> 16) * T + t];
+        const long long Gbw = G[(size_t)(q.z & 0xFFFF) * T + t], Gbs = G[(size_t)(q.z >> 16) * T + t];
+        // weaker: Gw - (Gaw - C0a) - (Gbw - C0b); stronger: (T0 - Gs)
+        // - (CTa - (Gas - C0a)) - (CTb - (Gbs - C0b)).
+        const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
+        const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+        if (scalar) {
+          v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
+        } else {
+          double res = pa * (double)Wn;
+          res += pb * (double)Lx;
+          v = (float)res;
+        }
+        if (tk.c != 0.0) {
+          const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+          v += (float)(pc * (double)eq);
+        }
+      }
+      if (fout) fv = (float)(pd * (double)F);
+    };
+    // Two hands per step: both hands' loads are issued before the stores.
+    int h = tid / T;
+    for (; h + HSTEP < hpp; h += 2 * HSTEP) {
+      float v0, f0, v1, f1;
+      value(h, v0, f0);
+      value(h + HSTEP, v1, f1);
+      out[h] = v0;
+      out[h + HSTEP] = v1;
+      if (fout) {
+        fout[h] = f0;
+        fout[h + HSTEP] = f1;
+      }
+    }
+    for (; h < hpp; h += HSTEP) {
+      float v0, f0;
+      value(h, v0, f0);
+      out[h] = v0;
+      if (fout) fout[h] = f0;
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// Elements per thread of the instantiated kernels (odd: a thread's 8-byte
+// prefixes of consecutive chunks fall on different banks).
+#define PANEL_ES(X) X(7) X(11) X(15) X(19) X(23) X(27) X(31)
+
+static int panel_e_for(int cstride, int T) {
+  const int chunks = PANEL_THREADS / T;
+#define PANEL_PICK(e_) \
+  if ((e_) * chunks >= cstride + 1) return e_;
+  PANEL_ES(PANEL_PICK)
+#undef PANEL_PICK
+  return 0;
+}
+
+size_t panel_terminal_smem(int hpo, int hpp, int cstride, int tstride, int T) {
+  return PanelSmem(hpo, hpp, cstride, tstride, T).total;
+}
+
+template <int T>
+static const void* panel_fn(int e) {
+  switch (e) {
+#define PANEL_CASE(e_) \
+  case e_:             \
+    return (const void*)panel_terminal_kernel<T, e_>;
+    PANEL_ES(PANEL_CASE)
+#undef PANEL_CASE
+  }
+  return nullptr;
+}
+
+static const void* panel_kernel(int T, int e) { return T == 8 ? panel_fn<8>(e) : T == 4 ? panel_fn<4>(e) : nullptr; }
+
+// Sets the kernel's shared-memory limit for terminals of T lanes; returns
+// the elements per thread (0 if the layout does not fit) and the blocks per
+// SM.
+int panel_terminal_setup(int hpo, int hpp, int cstride, int tstride, int T, int& blocks_per_sm) {
+  blocks_per_sm = 0;
+  const int e = panel_e_for(cstride, T);
+  const void* fn = panel_kernel(T, e);
+  if (!fn) return 0;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  const size_t smem = panel_terminal_smem(hpo, hpp, cstride, tstride, T);
+  if (smem > (size_t)optin) return 0;
+  // The limit is the device's opt-in maximum (a per-kernel setting shared by
+  // every handle and both traversers), not this footprint.
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) return 0;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, PANEL_THREADS, smem) != cudaSuccess || b <= 0) return 0;
+  blocks_per_sm = b;
+  return e;
+}
+
+void launch_panel_terminal(const FastArgs& A, const FastTask* tasks, const PanelD* panels, int npanels, int T, int e,
+                           int max_blocks, cudaStream_t s) {
+  if (npanels <= 0) return;
+  const int hpo = A.hp[A.p ^ 1], hpp = A.hp[A.p];
+  const size_t smem = panel_terminal_smem(hpo, hpp, A.cstride, A.tstride, T);
+  const int blocks = npanels < max_blocks ? npanels : max_blocks;
+  if (T == 8) {
+    switch (e) {
+#define PANEL_L8(e_)                                                                              \
+  case e_:                                                                                        \
+    panel_terminal_kernel<8, e_><<<blocks, PANEL_THREADS, smem, s>>>(A, tasks, panels, npanels); \
+    break;
+      PANEL_ES(PANEL_L8)
+#undef PANEL_L8
+    }
+  } else {
+    switch (e) {
+#define PANEL_L4(e_)                                                                              \
+  case e_:                                                                                        \
+    panel_terminal_kernel<4, e_><<<blocks, PANEL_THREADS, smem, s>>>(A, tasks, panels, npanels); \
+    break;
+      PANEL_ES(PANEL_L4)
+#undef PANEL_L4
+    }
+  }
+}
+
+}  // namespace dcfr

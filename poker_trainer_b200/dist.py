@@ -55,6 +55,15 @@ class Group:
             torch.cuda.synchronize(t.device)
         return t
 
+    def gather_concat(self, items: list) -> list:
+        """Every rank's list, concatenated in rank order, on rank 0 (other
+        ranks get []); the lists may differ in length."""
+        if self.dist is None:
+            return list(items)
+        out = [None] * self.world if self.rank == 0 else None
+        self.dist.gather_object(list(items), out, dst=0)
+        return [x for part in out for x in part] if self.rank == 0 else []
+
     def close(self):
         if self.dist is not None:
             self.dist.destroy_process_group()

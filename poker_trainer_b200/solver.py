@@ -29,6 +29,7 @@ EXPORTS = [
     "dcfr_actions_at", "dcfr_query_sizes", "dcfr_query", "dcfr_ranges_after", "dcfr_storage_len",
     "dcfr_download_storage", "dcfr_upload_storage", "dcfr_set_iterations", "dcfr_traverse",
     "dcfr_kernel_launches", "dcfr_last_iterate_ms", "dcfr_iteration_bytes", "dcfr_iterate_profiled",
+    "dcfr_terminal_kernel", "dcfr_last_solve_ms", "dcfr_setup_profile_get",
     "dcfr_showdown_values_noalloc", "dcfr_exploitability_fp64",
     "dcfr_batch_create", "dcfr_batch_destroy", "dcfr_batch_iterate", "dcfr_batch_exploitability",
     "dcfr_batch_storage_len", "dcfr_batch_download_storage", "dcfr_batch_autotune", "dcfr_batch_get_tuning",
@@ -99,6 +100,9 @@ def lib():
         L.dcfr_set_iterations.argtypes = [P, C.c_uint32]
         L.dcfr_traverse.argtypes = [P, C.c_int32, C.c_int32, C.c_uint32, P]
         L.dcfr_kernel_launches.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.dcfr_terminal_kernel.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.dcfr_last_solve_ms.argtypes = [P, C.POINTER(C.c_double)]
+        L.dcfr_setup_profile_get.argtypes = [P, C.POINTER(abi.SetupProfile)]
         L.dcfr_last_iterate_ms.argtypes = [P, C.POINTER(C.c_double)]
         L.dcfr_iteration_bytes.argtypes = [P, C.POINTER(C.c_double)]
         L.dcfr_iterate_profiled.argtypes = [P, C.c_uint32, C.POINTER(abi.KernelProfile)]
@@ -460,6 +464,27 @@ class Solver:
         out = np.zeros(self.num_hands(p), np.float32)
         check(lib().dcfr_traverse(self._h, p, mode, t, _ptr(out)))
         return out
+
+    def last_solve_ms(self) -> float:
+        """Device time of the last solve() (CUDA events on the handle's
+        stream around it), milliseconds."""
+        x = C.c_double()
+        check(lib().dcfr_last_solve_ms(self._h, C.byref(x)))
+        return x.value
+
+    def setup_profile(self) -> dict:
+        """Host milliseconds of each setup phase (dcfr_setup_profile)."""
+        sp = abi.SetupProfile()
+        check(lib().dcfr_setup_profile_get(self._h, C.byref(sp)))
+        return {f[0]: getattr(sp, f[0]) for f in abi.SetupProfile._fields_}
+
+    def terminal_kernel(self) -> tuple:
+        """(kernel name, terminals per panel) of this handle's f32 terminal
+        evaluation: "panel", "warp", "block" or "exact"."""
+        k = C.c_int32()
+        t = C.c_int32()
+        check(lib().dcfr_terminal_kernel(self._h, C.byref(k), C.byref(t)))
+        return ("panel", "warp", "block", "exact")[k.value], t.value
 
     def kernel_launches(self) -> int:
         x = C.c_uint64()

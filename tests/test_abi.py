@@ -44,6 +44,7 @@ STRUCTS = {
     "dcfr_tree_stats": abi.TreeStats, "dcfr_solve_options": abi.SolveOptions, "dcfr_progress": abi.Progress,
     "dcfr_step": abi.Step, "dcfr_action": abi.ActionT, "dcfr_node_info": abi.NodeInfoHeader,
     "dcfr_kernel_profile": abi.KernelProfile, "dcfr_batch_tuning": abi.BatchTuning,
+    "dcfr_setup_profile": abi.SetupProfile,
 }
 
 

@@ -152,3 +152,51 @@ def test_data_parallel_training_with_gloo():
     single = _OracleNet([5, 6, 3], seed=1)
     train(X, Y, M, steps=4, batch=16, lr=1e-2, seed=0, net=single, device="cpu")
     assert np.allclose(res[0][1], single.flat(), rtol=1e-10, atol=1e-12)
+
+
+def _spots():
+    from poker_trainer_b200 import workloads
+    return workloads.batched_river_spots(count=5, seed=3000)
+
+
+def _batch_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    from oracle_api import OracleSolver
+    g = Group(backend="gloo", timeout_s=60)
+    mine = shard(list(range(5)), g.rank, g.world)
+    spots = _spots()
+    expl = []
+    for i in mine:
+        o = OracleSolver(spots[i])
+        o.iterate(3)
+        expl.append((i, o.exploitability()))
+    got = g.gather_concat(expl)
+    out.put((rank, got))
+    g.close()
+
+
+def test_batch_spots_partitioned_and_gathered_with_gloo():
+    """The batched workload's multi-rank form (bench.py --workload batch):
+    the spots are partitioned across two ranks, each rank solves its own
+    (here with the CPU oracle), and rank 0 gathers every spot's
+    exploitability in spot order; each spot is solved exactly once and the
+    gathered values equal one process solving them all."""
+    from oracle_api import OracleSolver
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(out.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[1] == []
+    assert [i for i, _ in res[0]] == list(range(5))
+    for i, cfg in enumerate(_spots()):
+        o = OracleSolver(cfg)
+        o.iterate(3)
+        assert res[0][i][1] == o.exploitability()

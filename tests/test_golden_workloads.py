@@ -17,6 +17,9 @@ from poker_trainer_b200 import abi
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FIX = json.load(open(os.path.join(HERE, "workload_oracle.json")))
+# The flop entry holds 20 GB of storage in each solver: its bit-for-bit GPU
+# check lives in test_gpu_flop.py, and the CPU suite does not re-run it.
+SMALL_RUNS = [n for n in ORACLE_RUNS if n != "flop"]
 
 
 def committed_ranges():
@@ -31,7 +34,7 @@ def test_workload_ranges_match_fixture(name):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
-@pytest.mark.parametrize("name", list(ORACLE_RUNS))
+@pytest.mark.parametrize("name", SMALL_RUNS)
 def test_oracle_matches_fixture(name):
     from oracle_api import OracleSolver
 
@@ -44,7 +47,7 @@ def test_oracle_matches_fixture(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", list(ORACLE_RUNS))
+@pytest.mark.parametrize("name", SMALL_RUNS)
 def test_gpu_exact_matches_fixture(gpu, name):
     from poker_trainer_b200.solver import Solver
 
