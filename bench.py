@@ -790,29 +790,63 @@ def flop_paths(g, path=()):
 
 def run_learned(args, world, rank, local):
     """Config of the learned depth-limited flop solve: data from the GPU
-    solver, training on the library's tensor-core kernels, the depth-limited
-    solve against the full-tree solve, and the depth-limited flop strategy
-    evaluated inside the full tree by the FP64 best-response oracle."""
+    solver (turn subgames solved to 0.3% of the pot), networks trained on
+    growing prefixes of the data on the library's tensor-core kernels
+    (held-out error against training-set size), the depth-limited solve with
+    the largest network against the full-tree solve, and the depth-limited
+    flop strategy evaluated inside the full tree by the FP64 best-response
+    oracle. Data generation and training are reported as a one-time cost:
+    the same network serves every flop of this shape. With N GPUs the
+    subgames are partitioned across ranks (each solves its share) and the
+    network trains data-parallel; rank 0 runs the solves and reports."""
     import numpy as np
     import torch
     from poker_trainer_b200 import leafdata
+    from poker_trainer_b200.dist import Group
     from poker_trainer_b200.mlp import LeafNet, gemm_time
     from poker_trainer_b200.solver import Solver, SolveOptions
     from poker_trainer_b200.train_leaf import masked_mse, predict, train
 
     torch.cuda.set_device(local)
+    grp = Group("nccl", torch.device("cuda", local), timeout_s=3600)
     cfg = workload_config("flop", "fast")
     pot = float(cfg.root.pot)
+    sizes = sorted({int(x) for x in args.learned_sizes.split(",")} | {args.learned_samples}) \
+        if args.learned_sizes else [args.learned_samples]
+    sizes = [n for n in sizes if n <= args.learned_samples]
     t0 = time.perf_counter()
-    X, Y, M, _, iters = leafdata.make_dataset(args.learned_samples, seed=4000, target_pct=0.3, max_iterations=400)
-    Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(64, seed=5000, target_pct=0.3, max_iterations=400, with_equity=True)
-    t_data = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    net, losses = train(X, Y, M, hidden=1024, layers=4, steps=args.learned_steps, batch=256, lr=1e-3, seed=0)
+    X, Y, M, _, iters = leafdata.make_dataset(args.learned_samples, seed=4000, target_pct=0.3, max_iterations=400,
+                                              workers=args.learned_workers, part=(rank, world))
     torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    pred = predict(net, Xh)
-    mean = (Y * M).sum(0) / np.maximum(M.sum(0), 1.0)
+    t_data = grp.reduce(time.perf_counter() - t0, "max")
+    Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(64, seed=5000, target_pct=0.3, max_iterations=400, with_equity=True,
+                                              workers=args.learned_workers)
+    per_hand_mean = None
+    curve = []
+    net = None
+    t_train = 0.0
+    for n in sizes:
+        # The first n subgames of the seeded sequence (this rank's share of
+        # them under N ranks: samples r, r + N, ...).
+        k = len(range(rank, n, world))
+        steps = max(args.learned_steps, int(args.learned_steps * n / sizes[-1])) if n == sizes[-1] else \
+            max(1000, int(args.learned_steps * n / sizes[-1]))
+        t0 = time.perf_counter()
+        net_n, losses = train(X[:k], Y[:k], M[:k], hidden=1024, layers=4, steps=steps, batch=256, lr=1e-3, seed=0,
+                              group=grp if world > 1 else None, local=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        pred = predict(net_n, Xh)
+        mean = (Y[:k] * M[:k]).sum(0) / np.maximum(M[:k].sum(0), 1.0)
+        curve.append({"training_subgames": n, "steps": steps, "train_seconds": dt,
+                      "heldout_mse": masked_mse(pred, Yh, Mh),
+                      "heldout_mse_per_hand_mean": masked_mse(mean[None, :], Yh, Mh),
+                      "loss_last": float(np.mean(losses[-20:]))})
+        if n == sizes[-1]:
+            net, t_train, per_hand_mean = net_n, dt, masked_mse(mean[None, :], Yh, Mh)
+    if rank != 0:
+        grp.close()
+        return 0
     # The solve's network: same weights, batch room for every leaf x card.
     dlnet = LeafNet(leafdata.IN_DIM, 1024, 4, leafdata.OUT_DIM, max_batch=8192, seed=0)
     dlnet.set_params(net.params())
@@ -822,18 +856,12 @@ def run_learned(args, world, rank, local):
     gemm_tflops = 2.0 * 4096 * 2816 * 1024 / gemm_s / 1e12
     opts = SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10)
     full = Solver.new(cfg)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     pf = full.solve(opts)
-    full.synchronize()
-    t_full = time.perf_counter() - t0
+    t_full = full.last_solve_ms() / 1000.0
     e_full, _ = full.exploitability_fp64()
     dl = Solver.new_depth_limited(cfg, dlnet)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     pd = dl.solve(opts)
-    dl.synchronize()
-    t_dl = time.perf_counter() - t0
+    t_dl = dl.last_solve_ms() / 1000.0
     # Check: the depth-limited flop strategy inside the full tree.
     paths = flop_paths(dl)
     diffs = []
@@ -851,16 +879,36 @@ def run_learned(args, world, rank, local):
     # 1e20 x its probabilities: regret matching keeps playing it exactly
     # (what one iteration adds is below f32 resolution of those regrets, and
     # DCFR discounts all of a node's positive regrets by the same factor).
+    # The re-solve stops at the full solve's FP64 exploitability (or its
+    # iteration cap): equal quality, and the time that takes.
     lk = Solver.new(cfg)
     for path in paths:
         st = np.asarray(dl.query(path).strategy, np.float64)
         lk.write_node(path, regrets=(1e20 * st).astype(np.float32))
-    t0 = time.perf_counter()
-    plk = lk.solve(SolveOptions(max_iterations=args.lock_iterations, target_exploitability_pct=0.5, check_every=50))
-    lk.synchronize()
-    t_lock = time.perf_counter() - t0
+    target = max(100.0 * e_full / pot, 0.5)
+    plk = lk.solve(SolveOptions(max_iterations=args.lock_iterations, target_exploitability_pct=target,
+                                check_every=50))
+    t_lock = lk.last_solve_ms() / 1000.0
     e_lock, _ = lk.exploitability_fp64()
     lk.close()
+    # One turn subgame re-solved on the path played (check-check, then the
+    # As), the work a player of the depth-limited strategy does per turn
+    # reached: both ranges as they arrive at the cut under the depth-limited
+    # flop strategy, solved to 0.5% of the pot.
+    turn_resolve = None
+    try:
+        dlp = dl.ranges_after(["check", "check"])
+    except Exception:
+        dlp = None
+    if dlp is not None:
+        sub = leafdata.config_of(leafdata.abi.parse_cards("Ks7s2dAs"), int(pot), int(cfg.root.stack[0]),
+                                 [np.asarray(dlp[0], np.float32), np.asarray(dlp[1], np.float32)])
+        ts = Solver.new(sub)
+        pts = ts.solve(SolveOptions(max_iterations=1000, target_exploitability_pct=0.5, check_every=10))
+        turn_resolve = {"path": ["check", "check", "As"], "seconds": ts.last_solve_ms() / 1000.0,
+                        "iterations": pts.iteration, "exploitability_pct": pts.exploitability_pct}
+        ts.close()
+    dl.close()
     peak = 1672.6
     try:
         with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
@@ -868,11 +916,11 @@ def run_learned(args, world, rank, local):
     except (OSError, KeyError, ValueError):
         pass
     line = {
-        "metric": METRIC, "value": pd.iteration / t_dl, "unit": UNIT, "n_gpus": 1, "steps": pd.iteration,
-        "warmup": 0, "ms_per_step": 1000.0 * t_dl / max(pd.iteration, 1), "higher_is_better": True,
+        "metric": METRIC, "value": t_dl, "unit": "s", "n_gpus": world, "steps": pd.iteration,
+        "warmup": 0, "ms_per_step": 1000.0 * t_dl / max(pd.iteration, 1), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 solve, bf16 network (fp32 accumulation)",
         "data": "synthetic", "config": {"workload": WORKLOADS["learned"], "training_samples": args.learned_samples,
-                                        "training_steps": args.learned_steps},
+                                        "training_steps": args.learned_steps, "sizes": sizes},
         "time_to_target": {"full_tree_s": t_full, "full_tree_iterations": pf.iteration,
                            "full_tree_exploitability_pct_fp64": 100.0 * e_full / pot,
                            "depth_limited_s": t_dl, "depth_limited_iterations": pd.iteration,
@@ -880,18 +928,21 @@ def run_learned(args, world, rank, local):
                            "speedup": t_full / t_dl,
                            "depth_limited_flop_strategy_in_full_tree_exploitability_pct_fp64": 100.0 * e_comb / pot,
                            "flop_nodes": len(paths), "max_range_strategy_diff": max(diffs) if diffs else None,
+                           "locked_resolve_target_pct": target,
                            "depth_limited_flop_strategy_locked_resolve_exploitability_pct_fp64": 100.0 * e_lock / pot,
-                           "locked_resolve_iterations": plk.iteration, "locked_resolve_s": t_lock},
-        "training": {"data_seconds": t_data, "train_seconds": t_train, "solve_iterations_mean": float(np.mean(iters)),
-                     "loss_first": losses[0], "loss_last": float(np.mean(losses[-20:])),
-                     "heldout_mse": {"network": masked_mse(pred, Yh, Mh),
-                                     "per_hand_mean": masked_mse(mean[None, :], Yh, Mh),
-                                     "showdown_equity": masked_mse(Eh, Yh, Mh)}},
+                           "locked_resolve_iterations": plk.iteration, "locked_resolve_s": t_lock,
+                           "turn_resolve_on_path": turn_resolve},
+        "one_time_cost": {"data_seconds": t_data, "train_seconds": t_train,
+                          "subgames": args.learned_samples, "solve_iterations_mean": float(np.mean(iters)),
+                          "note": "paid once for every flop of this shape; not part of a solve"},
+        "training": {"curve": curve, "heldout_mse_showdown_equity": masked_mse(Eh, Yh, Mh),
+                     "heldout_mse_per_hand_mean": per_hand_mean},
         "roofline": {"bound": "tensor", "kernel": "gemm_bf16_tc_kernel (4096 x 1024 x 2816)", "achieved": gemm_tflops,
                      "peak": peak, "unit": "TFLOP/s", "frac": gemm_tflops / peak, "peak_kind": "of measured",
                      "traffic": None},
     }
     print(json.dumps(line), flush=True)
+    grp.close()
     return 0
 
 
@@ -917,7 +968,10 @@ def main():
     ap.add_argument("--cpu-flop-iters", type=int, default=3, help="flop: oracle iterations timed for the CPU figure")
     ap.add_argument("--cpu-batch-iters", type=int, default=20, help="batch: oracle iterations per spot timed")
     ap.add_argument("--learned-samples", type=int, default=1024, help="learned: solved turn subgames to train on")
-    ap.add_argument("--learned-steps", type=int, default=2000, help="learned: training steps")
+    ap.add_argument("--learned-steps", type=int, default=2000, help="learned: training steps (largest size)")
+    ap.add_argument("--learned-sizes", default=None, metavar="N1,N2,...",
+                    help="learned: also train on these prefixes of the data (held-out error against size)")
+    ap.add_argument("--learned-workers", type=int, default=4, help="learned: host threads solving subgames")
     ap.add_argument("--batch-tuning", default=None, metavar="WARPS,BLOCKS_PER_SM,ITERS_PER_LAUNCH,LONGEST_FIRST",
                     help="batch: a fixed launch shape instead of the autotuner's")
     ap.add_argument("--lock-iterations", type=int, default=300,

@@ -446,11 +446,12 @@ Status Engine::ensure_fast_layouts() {
     return s;
   }
   fast_blocks_ = sms * per_sm;
-  // The f32 solve's terminal kernel: panels of 8 terminals where that
-  // layout fits a block, else panels of 4; DCFR_TERMINAL_KERNEL selects
-  // another one (panel, panel4, panel8, warp, block) for comparisons.
+  // The f32 solve's terminal kernel: a warp per terminal for short hand
+  // lists, a block-wide scan per terminal for long ones (measured fastest);
+  // DCFR_TERMINAL_KERNEL selects another one (panel, panel4, panel8, warp,
+  // block) for comparisons.
   const char* sel = std::getenv("DCFR_TERMINAL_KERNEL");
-  const std::string want = sel ? sel : "panel";
+  const std::string want = sel ? sel : (tstride_ <= WARP_TERMINAL_MAX_HANDS ? "warp" : "block");
   term_kernel_ = want == "warp" ? TK_WARP : want == "block" ? TK_BLOCK : TK_PANEL;
   if (term_kernel_ == TK_PANEL) {
     const int o0 = 1, o1 = 0;  // opponent of traverser 0 and 1

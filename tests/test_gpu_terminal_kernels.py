@@ -1,14 +1,14 @@
 """The f32 solve's fast-precision terminal kernels against each other.
 
-The panel kernel (terminal_panel.cu, the default: 8 or 4 terminals of one
-board per block pass), the warp-per-terminal kernel and the block-scan
-kernel (terminal_fast.cu) evaluate the same exact integer prefix sums and
+The panel kernel (terminal_panel.cu: 8 or 4 terminals of one board per
+block pass), the warp-per-terminal kernel and the block-scan kernel
+(terminal_fast.cu, the defaults for short and long hand lists) evaluate the same exact integer prefix sums and
 round them with the same f64/f32 operations, so their results must agree
 bit for bit: traversal values from random storage in every mode, and the
 regrets, strategy sums and exploitability after iterations. The kernel is
 chosen per handle by DCFR_TERMINAL_KERNEL when the handle is created.
 Agreement with the CPU oracle itself is covered by test_gpu_fast.py and
-test_gpu_flop.py, which run the default (panel) kernel."""
+test_gpu_flop.py, which run the default kernels."""
 import numpy as np
 import pytest
 
@@ -81,8 +81,13 @@ def test_terminal_kernels_bit_identical(gpu, name, monkeypatch):
             assert same_bits(got[key], ref[key]), f"{name}: {kernel} differs from warp in {key}"
 
 
-def test_panel_is_the_default(gpu, monkeypatch):
+def test_default_kernel_by_hand_count(gpu, monkeypatch):
     monkeypatch.delenv("DCFR_TERMINAL_KERNEL", raising=False)
+    for make, want in ((workloads.turn_spot, ("block", 0)), (workloads.turn_narrow_spot, ("warp", 0))):
+        g = Solver.new(make())
+        assert g.terminal_kernel() == want
+        g.close()
+    monkeypatch.setenv("DCFR_TERMINAL_KERNEL", "panel")
     for make, width in ((workloads.turn_spot, 4), (workloads.turn_narrow_spot, 8)):
         g = Solver.new(make())
         assert g.terminal_kernel() == ("panel", width)
