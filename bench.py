@@ -363,6 +363,7 @@ def run_ours(args, world, rank, local):
     e2e_solver.iterate(K)
     e2e_solver.download_storage(out=out)
     t1 = time.perf_counter()
+    setup = e2e_solver.setup_profile()
     e2e_solver.close()
     e2e_s = reduce(t1 - t0, "max")
     h2d = C.sizeof(cfg)
@@ -447,6 +448,7 @@ def run_ours(args, world, rank, local):
         "clocks": clocks,
         "e2e": {"value": world * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
+                "setup_ms": setup,
                 "what": "dcfr_create from the host config + K iterations + regrets and sums read back into pinned "
                         "host memory, wall clock, max over ranks; bytes are the per-solve totals / K"},
         "gpu_launches": int(launches),

@@ -36,7 +36,7 @@ constexpr int PANEL_WARPS = PANEL_THREADS / 32;
 
 // Shared-memory layout of a block (every offset 16-byte aligned).
 struct PanelSmem {
-  size_t rows, g, cat, rec, same, seg, cs, wsum, wmax, total;
+  size_t rows, g, cat, rec, same, seg, bs, wsum, wmax, task, alive, total;
   int rstride;  // floats per staged row: hpo + 4 (16-byte rows; bank stagger)
   __host__ __device__ PanelSmem(int hpo, int hpp, int cstride, int tstride, int T) {
     auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
@@ -47,10 +47,12 @@ struct PanelSmem {
     rec = up16(cat + (size_t)cstride * 2);                     // [tstride] uint4
     same = up16(rec + (size_t)tstride * 16);                   // [hpp] u16
     seg = up16(same + (size_t)hpp * 2);                        // [FAST_SEGS] u16
-    cs = up16(seg + FAST_SEGS * 2);                            // [52][T] {start prefix, total}
-    wsum = up16(cs + (size_t)52 * T * 16);                     // [PANEL_WARPS][T] i64
-    wmax = up16(wsum + (size_t)PANEL_WARPS * T * 8);           // [PANEL_WARPS] f32
-    total = up16(wmax + (size_t)PANEL_WARPS * 4);
+    bs = up16(seg + FAST_SEGS * 2);                            // [FAST_SEGS][T] i64: prefix at each segment start
+    wsum = up16(bs + (size_t)FAST_SEGS * T * 8);               // [PANEL_WARPS][T] i64
+    wmax = up16(wsum + (size_t)PANEL_WARPS * T * 8);           // [2][T][PANEL_WARPS] f32 row-maximum partials
+    task = up16(wmax + (size_t)2 * T * PANEL_WARPS * 4);       // [3][T] FastTask (ring)
+    alive = up16(task + (size_t)3 * T * sizeof(FastTask));     // [2][T] u32
+    total = up16(alive + (size_t)2 * T * 4);
   }
 };
 
@@ -61,13 +63,17 @@ __device__ __forceinline__ void panel_cp16(void* dst, const void* src) {
 
 // One block per SM. Block b takes the contiguous panel range
 // [b N / G, (b+1) N / G) (panels are ordered by layout) and stages a
-// layout when its range enters it. Per panel, five block barriers:
-//   (A) the panel's rows have landed (cp.async) and the previous panel is done;
-//   (B) per-warp row maxima written (and a new layout staged);
+// layout when its range enters it. Per panel, three block barriers:
+//   (A) the previous panel is done; this panel's rows, row-maximum partials,
+//       liveness flags and the next panel's task records are in place;
 //   (C) per-warp scan totals written;
-//   (D) prefixes written;
-//   (E) per-card segment starts and totals written.
-// The next panel's rows are copied in (cp.async) while this one runs.
+//   (D) prefixes and segment-start prefixes written;
+// and one more where a new layout is staged. Nothing on the way waits for
+// global memory: task records come through a three-panel ring of
+// asynchronous copies, the next panel's rows are copied while this one
+// runs, and at the end of a panel every thread waits for its own copies of
+// the next rows and reduces their maxima (each thread reads only what it
+// copied), so the next panel starts with its scales ready.
 template <int T, int E>
 __global__ void __launch_bounds__(PANEL_THREADS, 1)
     panel_terminal_kernel(FastArgs A, const FastTask* __restrict__ tasks, const PanelD* __restrict__ panels,
@@ -82,9 +88,11 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
   uint4* srec = reinterpret_cast<uint4*>(smem_panel + Ls.rec);
   uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_panel + Ls.same);
   uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_panel + Ls.seg);
-  longlong2* cs = reinterpret_cast<longlong2*>(smem_panel + Ls.cs);
+  long long* bs = reinterpret_cast<long long*>(smem_panel + Ls.bs);
   long long* wsum = reinterpret_cast<long long*>(smem_panel + Ls.wsum);
   float* wmax = reinterpret_cast<float*>(smem_panel + Ls.wmax);
+  FastTask* ring = reinterpret_cast<FastTask*>(smem_panel + Ls.task);
+  uint32_t* salive = reinterpret_cast<uint32_t*>(smem_panel + Ls.alive);
   const int rstride = Ls.rstride;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -92,6 +100,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
   constexpr int CPW = 32 / T;                      // scan chunks per warp
   const int k0 = (warp * CPW + lane / T) * E;      // first layout element of this thread's chunk
   constexpr int HSTEP = PANEL_THREADS / T;         // hands per value pass
+  constexpr int TWORDS = (int)(sizeof(FastTask) / 16);
 
   const int b0 = (int)(((long long)blockIdx.x * npanels) / gridDim.x);
   const int b1 = (int)(((long long)(blockIdx.x + 1) * npanels) / gridDim.x);
@@ -101,46 +110,83 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
     const uint32_t sm = h < np ? A.same[h] : NONE32;
     ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
   }
-  // Rows of panel pi into buffer b: T x (hpo / 4) 16-byte copies; rows of
-  // dead subtrees (and missing tasks) are not copied.
-  auto prefetch = [&](int pi, int b) {
+  // Task records of panel pi into ring entry r (16-byte copies).
+  auto fetch_tasks = [&](int pi, int r) {
     const PanelD P = panels[pi];
+    if (tid < (int)P.count * TWORDS) {
+      const int tt = tid / TWORDS, w = tid - tt * TWORDS;
+      panel_cp16(reinterpret_cast<unsigned char*>(ring + r * T + tt) + 16 * w,
+                 reinterpret_cast<const unsigned char*>(tasks + P.first + tt) + 16 * w);
+    }
+  };
+  // Rows of panel pi (task records in ring entry r) into buffer b:
+  // T x (hpo / 4) 16-byte copies.
+  auto fetch_rows = [&](int pi, int r, int b) {
+    const int cnt = (int)panels[pi].count;
     const int per = hpo >> 2;
     float* dst = rows + (size_t)b * T * rstride;
-    for (int i = tid; i < (int)P.count * per; i += PANEL_THREADS) {
+    for (int i = tid; i < cnt * per; i += PANEL_THREADS) {
       const int tt = i / per, j = i - tt * per;
-      const uint32_t slot = tasks[P.first + tt].slot;
-      if (A.alive[slot] != 0)
-        panel_cp16(dst + (size_t)tt * rstride + 4 * j, A.reach + (size_t)slot * A.stride + 4 * j);
+      const uint32_t slot = ring[r * T + tt].slot;
+      panel_cp16(dst + (size_t)tt * rstride + 4 * j, A.reach + (size_t)slot * A.stride + 4 * j);
     }
-    cp_async_commit();
   };
-  prefetch(b0, 0);
+  // Per-warp maxima of the rows of panel pi in buffer b, from the 16-byte
+  // chunks this thread copied (fetch_rows' assignment), after its own
+  // cp.async wait: wmax[b][row][warp].
+  auto own_row_max = [&](int pi, int b) {
+    const int cnt = (int)panels[pi].count;
+    const int per = hpo >> 2;
+    const float* src = rows + (size_t)b * T * rstride;
+    float m[T];
+#pragma unroll
+    for (int tt = 0; tt < T; tt++) m[tt] = 0.0f;
+    for (int i = tid; i < cnt * per; i += PANEL_THREADS) {
+      const int tt = i / per, j = i - tt * per;
+      const float4 v = *reinterpret_cast<const float4*>(src + (size_t)tt * rstride + 4 * j);
+      const float mv = fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
+#pragma unroll
+      for (int u = 0; u < T; u++)
+        if (u == tt) m[u] = fmaxf(m[u], mv);
+    }
+#pragma unroll
+    for (int u = 0; u < T; u++) {
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) m[u] = fmaxf(m[u], __shfl_xor_sync(0xffffffffu, m[u], d));
+      if (lane == 0) wmax[(b * T + u) * PANEL_WARPS + warp] = m[u];
+    }
+  };
+  // Prologue: task records of the first two panels, then the first rows
+  // and their maxima.
+  fetch_tasks(b0, 0);
+  if (b0 + 1 < b1) fetch_tasks(b0 + 1, 1);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  if (tid < (int)panels[b0].count) salive[tid] = A.alive[ring[tid].slot];
+  fetch_rows(b0, 0, 0);
+  cp_async_commit();
+  cp_async_wait<0>();
+  own_row_max(b0, 0);
   uint32_t layout = NONE32;
   int L = 0;
+  int bfirst = 1;  // first segment start at or after this thread's chunk
 
   for (int pi = b0; pi < b1; pi++) {
-    const int buf = (pi - b0) & 1;
-    cp_async_wait<0>();
+    const int buf = (pi - b0) & 1, r = (pi - b0) % 3;
     __syncthreads();  // (A)
-    if (pi + 1 < b1) prefetch(pi + 1, buf ^ 1);
+    // The panel after next's task records, the next panel's rows, and the
+    // next panel's liveness flags (stored at the end of this panel).
+    uint32_t next_alive = 0;
+    if (pi + 1 < b1) {
+      if (pi + 2 < b1) fetch_tasks(pi + 2, (r + 2) % 3);
+      fetch_rows(pi + 1, (r + 1) % 3, buf ^ 1);
+      if (tid < (int)panels[pi + 1].count) next_alive = A.alive[ring[((r + 1) % 3) * T + tid].slot];
+    }
+    cp_async_commit();
     const PanelD P = panels[pi];
     const float* rbase = rows + (size_t)buf * T * rstride;
-    // Row maxima: warp w reduces part w / T of row w % T.
-    {
-      const int tt = warp % T, part = warp / T;
-      constexpr int PARTS = PANEL_WARPS / T;
-      const float4* r4 = reinterpret_cast<const float4*>(rbase + (size_t)tt * rstride);
-      float mx = 0.0f;
-      for (int i = part * 32 + lane; i < (hpo >> 2); i += 32 * PARTS) {
-        const float4 v = r4[i];
-        mx = fmaxf(mx, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
-      }
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-      if (lane == 0) wmax[warp] = mx;
-    }
-    if (P.layout != layout) {
+    if (P.layout != layout) {  // block-uniform
       layout = P.layout;
       const size_t lay = (size_t)layout * 2 + p;
       const uint16_t* gseg = A.seg + lay * FAST_SEGS;
@@ -150,16 +196,18 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
       for (int k = tid; k < Ln; k += PANEL_THREADS) scat[k] = gcat[k];
       const uint4* grec = A.rec + lay * A.tstride;
       for (int h = tid; h < np; h += PANEL_THREADS) srec[h] = grec[h];
+      __syncthreads();  // the new layout is staged
+      L = sseg[FAST_SEGS - 1];
+      bfirst = 1;
+      while (bfirst < FAST_SEGS && (int)sseg[bfirst] < k0) bfirst++;
     }
-    __syncthreads();  // (B)
-    L = sseg[FAST_SEGS - 1];
     // This thread's task (lane t of the panel).
     const bool has = t < (int)P.count;
-    const FastTask tk = tasks[P.first + (has ? t : 0)];
-    const bool live = has && A.alive[tk.slot] != 0;
+    const FastTask& tk = ring[r * T + (has ? t : 0)];
+    const bool live = has && salive[buf * T + t] != 0;
     float mx = 0.0f;
 #pragma unroll
-    for (int w = t; w < PANEL_WARPS; w += T) mx = fmaxf(mx, wmax[w]);
+    for (int w = 0; w < PANEL_WARPS; w++) mx = fmaxf(mx, wmax[(buf * T + t) * PANEL_WARPS + w]);
     const int S = scale_exponent(mx);
     const double scale = pow2(S), inv = pow2(-S);
     const float* myrow = rbase + (size_t)t * rstride;
@@ -185,83 +233,98 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
     __syncthreads();  // (C)
     long long acc = inc - local;
     for (int w = 0; w < warp; w++) acc += wsum[w * T + t];
+    // Prefixes, and the prefix at every segment start inside this chunk
+    // (segment j starts at sseg[j]; empty segments share a start).
+    int b = bfirst;
+    int nb = b < FAST_SEGS ? (int)sseg[b] : 0x7FFFFFFF;
 #pragma unroll
     for (int i = 0; i < E; i++) {
       const int k = k0 + i;
+      while (k == nb) {
+        bs[b * T + t] = acc;
+        b++;
+        nb = b < FAST_SEGS ? (int)sseg[b] : 0x7FFFFFFF;
+      }
       if (k <= L) G[(size_t)k * T + t] = acc;
       acc += x[i];
     }
     __syncthreads();  // (D)
-    for (int i = tid; i < 52 * T; i += PANEL_THREADS) {
-      const int c = i / T, tt = i - c * T;
-      const long long s0 = G[(size_t)sseg[1 + c] * T + tt];
-      cs[i] = make_longlong2(s0, G[(size_t)sseg[2 + c] * T + tt] - s0);
-    }
-    __syncthreads();  // (E)
 
-    if (!live) continue;  // dead subtree (cfr.rs:267-274) or no task: rows untouched
-    const uint32_t kind = tk.kind;
-    const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
-    const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
-    const double pa = tk.a * inv, pb = tk.b * inv, pc = tk.c * inv, pd = tk.d * inv;
-    const long long T0 = G[(size_t)sseg[1] * T + t];
-    float* out = A.vals + (size_t)tk.row * A.stride;
-    float* fout = tk.frow != NONE32 ? A.vals + (size_t)tk.frow * A.stride : nullptr;
-    auto value = [&](int h, float& v, float& fv) {
-      v = 0.0f;
-      fv = 0.0f;
-      if (h >= np) return;
-      const uint4 q = srec[h];
-      const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
-      const longlong2 ca = cs[a * T + t], cb = cs[b * T + t];
-      const uint16_t sm = ssame[h];
-      const long long si = sm == 0xFFFF ? 0ll : fixed(myrow[sm], scale);
-      const long long F = T0 - ca.y - cb.y + si;
-      if (fold) {
-        // eval_fold (eval.rs:40-64) returns zeros on a zero total.
-        v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
-        return;
-      }
-      if (q.w >> 16) {
-        const long long Gw = G[(size_t)(q.x & 0xFFFF) * T + t], Gs = G[(size_t)(q.x >> 16) * T + t];
-        const long long Gaw = G[(size_t)(q.y & 0xFFFF) * T + t], Gas = G[(size_t)(q.y >> 16) * T + t];
-        const long long Gbw = G[(size_t)(q.z & 0xFFFF) * T + t], Gbs = G[(size_t)(q.z >> 16) * T + t];
-        // weaker: Gw - (Gaw - C0a) - (Gbw - C0b); stronger: (T0 - Gs)
-        // - (CTa - (Gas - C0a)) - (CTb - (Gbs - C0b)).
-        const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
-        const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
-        if (scalar) {
-          v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
-        } else {
-          double res = pa * (double)Wn;
-          res += pb * (double)Lx;
-          v = (float)res;
+    if (live) {
+      const uint32_t kind = tk.kind;
+      const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
+      const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
+      const double pa = tk.a * inv, pb = tk.b * inv, pc = tk.c * inv, pd = tk.d * inv;
+      const bool tie = tk.c != 0.0;
+      const long long T0 = bs[1 * T + t];
+      float* out = A.vals + (size_t)tk.row * A.stride;
+      float* fout = tk.frow != NONE32 ? A.vals + (size_t)tk.frow * A.stride : nullptr;
+      auto value = [&](int h, float& v, float& fv) {
+        v = 0.0f;
+        fv = 0.0f;
+        if (h >= np) return;
+        const uint4 q = srec[h];
+        const int a = (int)(q.w & 0xFF), bb = (int)((q.w >> 8) & 0xFF);
+        const long long a0 = bs[(1 + a) * T + t], b0_ = bs[(1 + bb) * T + t];
+        const longlong2 ca = make_longlong2(a0, bs[(2 + a) * T + t] - a0);
+        const longlong2 cb = make_longlong2(b0_, bs[(2 + bb) * T + t] - b0_);
+        const uint16_t sm = ssame[h];
+        const long long si = sm == 0xFFFF ? 0ll : fixed(myrow[sm], scale);
+        const long long F = T0 - ca.y - cb.y + si;
+        if (fold) {
+          // eval_fold (eval.rs:40-64) returns zeros on a zero total.
+          v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
+          return;
         }
-        if (tk.c != 0.0) {
-          const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
-          v += (float)(pc * (double)eq);
+        if (q.w >> 16) {
+          const long long Gw = G[(size_t)(q.x & 0xFFFF) * T + t], Gs = G[(size_t)(q.x >> 16) * T + t];
+          const long long Gaw = G[(size_t)(q.y & 0xFFFF) * T + t], Gas = G[(size_t)(q.y >> 16) * T + t];
+          const long long Gbw = G[(size_t)(q.z & 0xFFFF) * T + t], Gbs = G[(size_t)(q.z >> 16) * T + t];
+          // weaker: Gw - (Gaw - C0a) - (Gbw - C0b); stronger: (T0 - Gs)
+          // - (CTa - (Gas - C0a)) - (CTb - (Gbs - C0b)).
+          const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
+          const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+          if (scalar) {
+            v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
+          } else {
+            double res = pa * (double)Wn;
+            res += pb * (double)Lx;
+            v = (float)res;
+          }
+          if (tie) {
+            const long long eq = (Gs - Gw) - (Gas - Gaw) - (Gbs - Gbw) + si;
+            v += (float)(pc * (double)eq);
+          }
+        }
+        if (fout) fv = (float)(pd * (double)F);
+      };
+      // Two hands per step: both hands' loads are issued before the stores.
+      int h = tid / T;
+      for (; h + HSTEP < hpp; h += 2 * HSTEP) {
+        float v0, f0, v1, f1;
+        value(h, v0, f0);
+        value(h + HSTEP, v1, f1);
+        out[h] = v0;
+        out[h + HSTEP] = v1;
+        if (fout) {
+          fout[h] = f0;
+          fout[h + HSTEP] = f1;
         }
       }
-      if (fout) fv = (float)(pd * (double)F);
-    };
-    // Two hands per step: both hands' loads are issued before the stores.
-    int h = tid / T;
-    for (; h + HSTEP < hpp; h += 2 * HSTEP) {
-      float v0, f0, v1, f1;
-      value(h, v0, f0);
-      value(h + HSTEP, v1, f1);
-      out[h] = v0;
-      out[h + HSTEP] = v1;
-      if (fout) {
-        fout[h] = f0;
-        fout[h + HSTEP] = f1;
+      for (; h < hpp; h += HSTEP) {
+        float v0, f0;
+        value(h, v0, f0);
+        out[h] = v0;
+        if (fout) fout[h] = f0;
       }
     }
-    for (; h < hpp; h += HSTEP) {
-      float v0, f0;
-      value(h, v0, f0);
-      out[h] = v0;
-      if (fout) fout[h] = f0;
+    // Dead subtree (cfr.rs:267-274) or no task: rows untouched.
+    // The next panel: its rows (this thread's copies) and their maxima, and
+    // its liveness flags.
+    cp_async_wait<0>();
+    if (pi + 1 < b1) {
+      own_row_max(pi + 1, buf ^ 1);
+      if (tid < (int)panels[pi + 1].count) salive[(buf ^ 1) * T + tid] = next_alive;
     }
   }
   cp_async_wait<0>();
