@@ -34,21 +34,26 @@ namespace dcfr {
 constexpr int PANEL_THREADS = 512;
 constexpr int PANEL_WARPS = PANEL_THREADS / 32;
 
-// Shared-memory layout of a block (every offset 16-byte aligned).
+// Shared-memory layout of a block (every offset 16-byte aligned). E x
+// (threads / T) scan positions: the layout padded past its end, so the scan
+// needs no bounds test.
 struct PanelSmem {
-  size_t rows, g, cat, rec, same, seg, bs, wsum, wmax, task, alive, total;
+  size_t rows, g, cat, rec, same, seg, pairs, t0, wsum, wmax, task, alive, total;
   int rstride;  // floats per staged row: hpo + 4 (16-byte rows; bank stagger)
-  __host__ __device__ PanelSmem(int hpo, int hpp, int cstride, int tstride, int T) {
+  int npos;     // scan positions
+  __host__ __device__ PanelSmem(int hpo, int hpp, int tstride, int T, int E) {
     auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
     rstride = hpo + 4;
+    npos = E * (PANEL_THREADS / T);
     rows = 0;                                                  // [2][T][rstride] f32
-    g = up16(rows + (size_t)2 * T * rstride * 4);              // [cstride + 1][T] i64
-    cat = up16(g + ((size_t)cstride + 1) * T * 8);             // [cstride] u16
-    rec = up16(cat + (size_t)cstride * 2);                     // [tstride] uint4
+    g = up16(rows + (size_t)2 * T * rstride * 4);              // [npos][T] i64
+    cat = up16(g + (size_t)npos * T * 8);                      // [npos] u16
+    rec = up16(cat + (size_t)npos * 2);                        // [tstride] uint4
     same = up16(rec + (size_t)tstride * 16);                   // [hpp] u16
     seg = up16(same + (size_t)hpp * 2);                        // [FAST_SEGS] u16
-    bs = up16(seg + FAST_SEGS * 2);                            // [FAST_SEGS][T] i64: prefix at each segment start
-    wsum = up16(bs + (size_t)FAST_SEGS * T * 8);               // [PANEL_WARPS][T] i64
+    pairs = up16(seg + FAST_SEGS * 2);                         // [52][T] {prefix at card segment start, at end}
+    t0 = up16(pairs + (size_t)52 * T * 16);                    // [T] i64: the main segment's total
+    wsum = up16(t0 + (size_t)T * 8);                           // [PANEL_WARPS][T] i64
     wmax = up16(wsum + (size_t)PANEL_WARPS * T * 8);           // [2][T][PANEL_WARPS] f32 row-maximum partials
     task = up16(wmax + (size_t)2 * T * PANEL_WARPS * 4);       // [3][T] FastTask (ring)
     alive = up16(task + (size_t)3 * T * sizeof(FastTask));     // [2][T] u32
@@ -67,7 +72,7 @@ __device__ __forceinline__ void panel_cp16(void* dst, const void* src) {
 //   (A) the previous panel is done; this panel's rows, row-maximum partials,
 //       liveness flags and the next panel's task records are in place;
 //   (C) per-warp scan totals written;
-//   (D) prefixes and segment-start prefixes written;
+//   (D) prefixes and segment-boundary prefixes written;
 // and one more where a new layout is staged. Nothing on the way waits for
 // global memory: task records come through a three-panel ring of
 // asynchronous copies, the next panel's rows are copied while this one
@@ -81,26 +86,29 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
   extern __shared__ __align__(16) unsigned char smem_panel[];
   const int p = A.p, o = p ^ 1;
   const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
-  const PanelSmem Ls(hpo, hpp, A.cstride, A.tstride, T);
+  const PanelSmem Ls(hpo, hpp, A.tstride, T, E);
   float* rows = reinterpret_cast<float*>(smem_panel + Ls.rows);
   long long* G = reinterpret_cast<long long*>(smem_panel + Ls.g);
   uint16_t* scat = reinterpret_cast<uint16_t*>(smem_panel + Ls.cat);
   uint4* srec = reinterpret_cast<uint4*>(smem_panel + Ls.rec);
   uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_panel + Ls.same);
   uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_panel + Ls.seg);
-  long long* bs = reinterpret_cast<long long*>(smem_panel + Ls.bs);
+  longlong2* pairs = reinterpret_cast<longlong2*>(smem_panel + Ls.pairs);
+  long long* pairs_ll = reinterpret_cast<long long*>(smem_panel + Ls.pairs);
+  long long* st0 = reinterpret_cast<long long*>(smem_panel + Ls.t0);
   long long* wsum = reinterpret_cast<long long*>(smem_panel + Ls.wsum);
   float* wmax = reinterpret_cast<float*>(smem_panel + Ls.wmax);
   FastTask* ring = reinterpret_cast<FastTask*>(smem_panel + Ls.task);
   uint32_t* salive = reinterpret_cast<uint32_t*>(smem_panel + Ls.alive);
-  const int rstride = Ls.rstride;
+  const int rstride = Ls.rstride, npos = Ls.npos;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t = lane % T;                          // this thread's terminal within a panel
   constexpr int CPW = 32 / T;                      // scan chunks per warp
-  const int k0 = (warp * CPW + lane / T) * E;      // first layout element of this thread's chunk
+  const int k0 = (warp * CPW + lane / T) * E;      // first layout position of this thread's chunk
   constexpr int HSTEP = PANEL_THREADS / T;         // hands per value pass
   constexpr int TWORDS = (int)(sizeof(FastTask) / 16);
+  const int per = hpo >> 2;                        // 16-byte chunks per row
 
   const int b0 = (int)(((long long)blockIdx.x * npanels) / gridDim.x);
   const int b1 = (int)(((long long)(blockIdx.x + 1) * npanels) / gridDim.x);
@@ -119,41 +127,34 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
                  reinterpret_cast<const unsigned char*>(tasks + P.first + tt) + 16 * w);
     }
   };
-  // Rows of panel pi (task records in ring entry r) into buffer b:
-  // T x (hpo / 4) 16-byte copies.
+  // Rows of panel pi (task records in ring entry r) into buffer b: thread
+  // tid copies chunks j = tid, tid + threads, ... of every row.
   auto fetch_rows = [&](int pi, int r, int b) {
     const int cnt = (int)panels[pi].count;
-    const int per = hpo >> 2;
     float* dst = rows + (size_t)b * T * rstride;
-    for (int i = tid; i < cnt * per; i += PANEL_THREADS) {
-      const int tt = i / per, j = i - tt * per;
-      const uint32_t slot = ring[r * T + tt].slot;
-      panel_cp16(dst + (size_t)tt * rstride + 4 * j, A.reach + (size_t)slot * A.stride + 4 * j);
-    }
+#pragma unroll
+    for (int tt = 0; tt < T; tt++)
+      if (tt < cnt) {
+        const float* src = A.reach + (size_t)ring[r * T + tt].slot * A.stride;
+        for (int j = tid; j < per; j += PANEL_THREADS) panel_cp16(dst + (size_t)tt * rstride + 4 * j, src + 4 * j);
+      }
   };
-  // Per-warp maxima of the rows of panel pi in buffer b, from the 16-byte
-  // chunks this thread copied (fetch_rows' assignment), after its own
-  // cp.async wait: wmax[b][row][warp].
+  // Per-warp maxima of the rows of panel pi in buffer b, from the chunks
+  // this thread copied, after its own cp.async wait: wmax[b][row][warp].
   auto own_row_max = [&](int pi, int b) {
     const int cnt = (int)panels[pi].count;
-    const int per = hpo >> 2;
     const float* src = rows + (size_t)b * T * rstride;
-    float m[T];
 #pragma unroll
-    for (int tt = 0; tt < T; tt++) m[tt] = 0.0f;
-    for (int i = tid; i < cnt * per; i += PANEL_THREADS) {
-      const int tt = i / per, j = i - tt * per;
-      const float4 v = *reinterpret_cast<const float4*>(src + (size_t)tt * rstride + 4 * j);
-      const float mv = fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w));
+    for (int tt = 0; tt < T; tt++) {
+      float m = 0.0f;
+      if (tt < cnt)
+        for (int j = tid; j < per; j += PANEL_THREADS) {
+          const float4 v = *reinterpret_cast<const float4*>(src + (size_t)tt * rstride + 4 * j);
+          m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+        }
 #pragma unroll
-      for (int u = 0; u < T; u++)
-        if (u == tt) m[u] = fmaxf(m[u], mv);
-    }
-#pragma unroll
-    for (int u = 0; u < T; u++) {
-#pragma unroll
-      for (int d = 16; d > 0; d >>= 1) m[u] = fmaxf(m[u], __shfl_xor_sync(0xffffffffu, m[u], d));
-      if (lane == 0) wmax[(b * T + u) * PANEL_WARPS + warp] = m[u];
+      for (int d = 16; d > 0; d >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, d));
+      if (lane == 0) wmax[(b * T + tt) * PANEL_WARPS + warp] = m;
     }
   };
   // Prologue: task records of the first two panels, then the first rows
@@ -169,8 +170,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
   cp_async_wait<0>();
   own_row_max(b0, 0);
   uint32_t layout = NONE32;
-  int L = 0;
-  int bfirst = 1;  // first segment start at or after this thread's chunk
+  int bfirst = 1;  // first segment boundary at or after this thread's chunk
 
   for (int pi = b0; pi < b1; pi++) {
     const int buf = (pi - b0) & 1, r = (pi - b0) % 3;
@@ -193,11 +193,12 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
       if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
       const int Ln = gseg[FAST_SEGS - 1];
       const uint16_t* gcat = A.cat + lay * A.cstride;
-      for (int k = tid; k < Ln; k += PANEL_THREADS) scat[k] = gcat[k];
+      // Positions past the layout's end read hand 0: their sums only reach
+      // prefixes beyond the end, which nothing reads.
+      for (int k = tid; k < npos; k += PANEL_THREADS) scat[k] = k < Ln ? gcat[k] : (uint16_t)0;
       const uint4* grec = A.rec + lay * A.tstride;
       for (int h = tid; h < np; h += PANEL_THREADS) srec[h] = grec[h];
       __syncthreads();  // the new layout is staged
-      L = sseg[FAST_SEGS - 1];
       bfirst = 1;
       while (bfirst < FAST_SEGS && (int)sseg[bfirst] < k0) bfirst++;
     }
@@ -212,16 +213,13 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
     const double scale = pow2(S), inv = pow2(-S);
     const float* myrow = rbase + (size_t)t * rstride;
 
-    // Scan: E consecutive elements per thread, held in registers.
+    // Scan: E consecutive positions per thread, held in registers.
     long long x[E];
     long long local = 0;
 #pragma unroll
     for (int i = 0; i < E; i++) {
-      const int k = k0 + i;
-      long long v = 0;
-      if (live && k < L) v = fixed(myrow[scat[k]], scale);
-      x[i] = v;
-      local += v;
+      x[i] = fixed(myrow[scat[k0 + i]], scale);
+      local += x[i];
     }
     long long inc = local;
 #pragma unroll
@@ -231,22 +229,33 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
     }
     if (lane >= 32 - T) wsum[warp * T + t] = inc;
     __syncthreads();  // (C)
-    long long acc = inc - local;
-    for (int w = 0; w < warp; w++) acc += wsum[w * T + t];
-    // Prefixes, and the prefix at every segment start inside this chunk
-    // (segment j starts at sseg[j]; empty segments share a start).
-    int b = bfirst;
-    int nb = b < FAST_SEGS ? (int)sseg[b] : 0x7FFFFFFF;
+    // The totals of the warps before this one, for this lane's terminal:
+    // lane l reads entries l, l + 32, ... ([warp][T], so all of terminal
+    // l % T), then the lanes of one terminal sum theirs.
+    long long before = 0;
+#pragma unroll
+    for (int q = 0; q < PANEL_WARPS * T / 32; q++) {
+      const int idx = lane + 32 * q;
+      if (idx / T < warp) before += wsum[idx];
+    }
+#pragma unroll
+    for (int d = T; d < 32; d <<= 1) before += __shfl_xor_sync(0xffffffffu, before, d);
+    long long acc = inc - local + before;
 #pragma unroll
     for (int i = 0; i < E; i++) {
-      const int k = k0 + i;
-      while (k == nb) {
-        bs[b * T + t] = acc;
-        b++;
-        nb = b < FAST_SEGS ? (int)sseg[b] : 0x7FFFFFFF;
-      }
-      if (k <= L) G[(size_t)k * T + t] = acc;
+      G[(size_t)(k0 + i) * T + t] = acc;
       acc += x[i];
+    }
+    // Segment boundaries inside this chunk (read back from this thread's own
+    // prefixes): card c's segment runs from boundary 1 + c to 2 + c, and
+    // boundary 1 closes the main segment.
+    for (int b = bfirst; b < FAST_SEGS; b++) {
+      const int kb = sseg[b];
+      if (kb >= k0 + E) break;
+      const long long pb = G[(size_t)kb * T + t];
+      if (b == 1) st0[t] = pb;
+      if (b <= 52) pairs_ll[((b - 1) * T + t) * 2] = pb;
+      if (b >= 2) pairs_ll[((b - 2) * T + t) * 2 + 1] = pb;
     }
     __syncthreads();  // (D)
 
@@ -256,34 +265,36 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
       const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
       const double pa = tk.a * inv, pb = tk.b * inv, pc = tk.c * inv, pd = tk.d * inv;
       const bool tie = tk.c != 0.0;
-      const long long T0 = bs[1 * T + t];
+      const long long T0 = st0[t];
       float* out = A.vals + (size_t)tk.row * A.stride;
       float* fout = tk.frow != NONE32 ? A.vals + (size_t)tk.frow * A.stride : nullptr;
+      const long long* Gt = G + t;
       auto value = [&](int h, float& v, float& fv) {
         v = 0.0f;
         fv = 0.0f;
         if (h >= np) return;
         const uint4 q = srec[h];
         const int a = (int)(q.w & 0xFF), bb = (int)((q.w >> 8) & 0xFF);
-        const long long a0 = bs[(1 + a) * T + t], b0_ = bs[(1 + bb) * T + t];
-        const longlong2 ca = make_longlong2(a0, bs[(2 + a) * T + t] - a0);
-        const longlong2 cb = make_longlong2(b0_, bs[(2 + bb) * T + t] - b0_);
+        // Card a's segment: prefix at its start (sa) and end (ea).
+        const longlong2 ca = pairs[a * T + t], cb = pairs[bb * T + t];
+        const long long sab = ca.x + cb.x, base = T0 - (ca.y + cb.y);
         const uint16_t sm = ssame[h];
         const long long si = sm == 0xFFFF ? 0ll : fixed(myrow[sm], scale);
-        const long long F = T0 - ca.y - cb.y + si;
+        // fold: T - (card a total) - (card b total) + identical hand.
+        const long long F = base + sab + si;
         if (fold) {
           // eval_fold (eval.rs:40-64) returns zeros on a zero total.
           v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
           return;
         }
         if (q.w >> 16) {
-          const long long Gw = G[(size_t)(q.x & 0xFFFF) * T + t], Gs = G[(size_t)(q.x >> 16) * T + t];
-          const long long Gaw = G[(size_t)(q.y & 0xFFFF) * T + t], Gas = G[(size_t)(q.y >> 16) * T + t];
-          const long long Gbw = G[(size_t)(q.z & 0xFFFF) * T + t], Gbs = G[(size_t)(q.z >> 16) * T + t];
-          // weaker: Gw - (Gaw - C0a) - (Gbw - C0b); stronger: (T0 - Gs)
-          // - (CTa - (Gas - C0a)) - (CTb - (Gbs - C0b)).
-          const long long Wn = (Gw + ca.x + cb.x) - Gaw - Gbw;
-          const long long Lx = (T0 + Gas + Gbs) - Gs - (ca.x + ca.y) - (cb.x + cb.y);
+          const long long Gw = Gt[(q.x & 0xFFFF) * T], Gs = Gt[(q.x >> 16) * T];
+          const long long Gaw = Gt[(q.y & 0xFFFF) * T], Gas = Gt[(q.y >> 16) * T];
+          const long long Gbw = Gt[(q.z & 0xFFFF) * T], Gbs = Gt[(q.z >> 16) * T];
+          // weaker: Gw - (Gaw - sa) - (Gbw - sb); stronger: (T0 - Gs)
+          // - (ea - Gas) - (eb - Gbs).
+          const long long Wn = (Gw + sab) - Gaw - Gbw;
+          const long long Lx = (base + Gas + Gbs) - Gs;
           if (scalar) {
             v = (float)(pa * (double)Wn) + (float)(pb * (double)Lx);
           } else {
@@ -344,7 +355,7 @@ static int panel_e_for(int cstride, int T) {
 }
 
 size_t panel_terminal_smem(int hpo, int hpp, int cstride, int tstride, int T) {
-  return PanelSmem(hpo, hpp, cstride, tstride, T).total;
+  return PanelSmem(hpo, hpp, tstride, T, panel_e_for(cstride, T)).total;
 }
 
 template <int T>
