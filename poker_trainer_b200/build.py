@@ -32,7 +32,7 @@ FLAGS = [
     "-Xcompiler", "-fPIC,-O3,-ffp-contract=off",
     "-ccbin", "g++",
 ]
-LINK = [*ARCH, "-ccbin", "g++", "--shared", "-cudart", "shared"]
+LINK = [*ARCH, "-ccbin", "g++", "--shared", "-cudart", "shared", "-lpthread"]
 
 
 def _mtime(path: str) -> float:

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <thread>
 #include <unordered_map>
 
 namespace dcfr {
@@ -371,11 +372,18 @@ Status Engine::init() {
     if (fast_ && !(s = ensure_fast_layouts()).ok()) return s;
   }
   phase(setup.tables_ms);
-  // Plans for the two traversals of an iteration.
-  for (int p = 0; p < 2; p++) {
-    full_[p].reset(new Plan());
-    if (!(s = build_plan(0, p, *full_[p])).ok()) return s;
-    max_slots_ = std::max<uint64_t>(max_slots_, full_[p]->nslots);
+  // Plans for the two traversals of an iteration, built concurrently on two
+  // host threads (build_plan only reads the game and the engine's layouts).
+  {
+    Status ps[2];
+    for (int p = 0; p < 2; p++) full_[p].reset(new Plan());
+    std::thread other([&]() { ps[1] = build_plan(0, 1, *full_[1]); });
+    ps[0] = build_plan(0, 0, *full_[0]);
+    other.join();
+    for (int p = 0; p < 2; p++) {
+      if (!ps[p].ok()) return ps[p];
+      max_slots_ = std::max<uint64_t>(max_slots_, full_[p]->nslots);
+    }
   }
   phase(setup.plans_ms);
   // Rows.
@@ -811,42 +819,60 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       u = g.nodes[u].parent;
     }
   }
-  std::vector<std::vector<FastTask>> by_sd(nb + 1), by_fold(nb + 1);
-  for (const SdLane& x : sd) {
-    const TermLane& L = x.lane;
-    by_sd[x.board].push_back(FastTask{x.kind, x.board, L.slot, L.row, L.frow, {0, 0, 0}, L.a, L.b, L.c, L.d});
+  // Each fold's layout, then per layout the showdowns' and folds' indices
+  // (counting sort: the tasks themselves are written once, in final order).
+  std::vector<uint32_t> fold_layout(folds[0].size() + folds[1].size(), nb);
+  for (size_t i = 0; i < folds[1].size(); i++)
+    for (uint32_t u = g.nodes[folds[1][i].row].parent; u != NO && g.nodes[u].kind == N_PLAYER;
+         u = g.nodes[u].parent)
+      if (seg_board[u] != NONE32) {
+        fold_layout[folds[0].size() + i] = seg_board[u];
+        break;
+      }
+  std::vector<uint32_t> s_off(nb + 2, 0), f_off(nb + 2, 0);
+  for (const SdLane& x : sd) s_off[x.board + 1]++;
+  for (uint32_t l : fold_layout) f_off[l + 1]++;
+  for (uint32_t l = 0; l <= nb; l++) {
+    s_off[l + 1] += s_off[l];
+    f_off[l + 1] += f_off[l];
   }
-  for (int b = 0; b < 2; b++)
-    for (const TermLane& L : folds[b]) {
-      uint32_t layout = nb;
-      if (b)
-        for (uint32_t u = g.nodes[L.row].parent; u != NO && g.nodes[u].kind == N_PLAYER; u = g.nodes[u].parent)
-          if (seg_board[u] != NONE32) {
-            layout = seg_board[u];
-            break;
-          }
-      by_fold[layout].push_back(FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, layout, L.slot, L.row,
-                                         NONE32, {0, 0, 0}, L.a, 0.0, 0.0, 0.0});
-    }
+  std::vector<uint32_t> s_idx(sd.size()), f_idx(fold_layout.size());
+  {
+    std::vector<uint32_t> fill(s_off.begin(), s_off.end() - 1);
+    for (size_t i = 0; i < sd.size(); i++) s_idx[fill[sd[i].board]++] = (uint32_t)i;
+    std::vector<uint32_t> ffill(f_off.begin(), f_off.end() - 1);
+    for (size_t i = 0; i < fold_layout.size(); i++) f_idx[ffill[fold_layout[i]]++] = (uint32_t)i;
+  }
+  auto sd_task = [&](uint32_t i) {
+    const SdLane& x = sd[i];
+    const TermLane& L = x.lane;
+    return FastTask{x.kind, x.board, L.slot, L.row, L.frow, {0, 0, 0}, L.a, L.b, L.c, L.d};
+  };
+  auto fold_task = [&](uint32_t i) {
+    const bool b = i >= folds[0].size();
+    const TermLane& L = b ? folds[1][i - folds[0].size()] : folds[0][i];
+    return FastTask{b ? (uint32_t)T_FOLD_BATCH : (uint32_t)T_FOLD_SCALAR, fold_layout[i], L.slot, L.row, NONE32,
+                    {0, 0, 0}, L.a, 0.0, 0.0, 0.0};
+  };
   // Within a layout, showdowns and folds are interleaved evenly in chunks of
   // PT tasks (after k chunks, about k |S| / (|S| + |F|) showdown chunks).
   // With the panel kernel a chunk is a panel, all showdowns or all folds.
   plan.h_fast.clear();
+  plan.h_fast.reserve(sd.size() + fold_layout.size());
   plan.h_panels.clear();
   const bool panels = fast_ && term_kernel_ == TK_PANEL;
   const size_t PT = panels ? (size_t)panel_T_ : 1;
   for (uint32_t l = 0; l <= nb; l++) {
-    const std::vector<FastTask>& S = by_sd[l];
-    const std::vector<FastTask>& F = by_fold[l];
-    const size_t ns = (S.size() + PT - 1) / PT, nf = (F.size() + PT - 1) / PT;
+    const size_t S0 = s_off[l], SN = s_off[l + 1] - S0, F0 = f_off[l], FN = f_off[l + 1] - F0;
+    const size_t ns = (SN + PT - 1) / PT, nf = (FN + PT - 1) / PT;
     size_t i = 0, j = 0;
     while (i < ns || j < nf) {
       const bool take_s = j >= nf || (i < ns && i * nf <= j * ns);
-      const std::vector<FastTask>& V = take_s ? S : F;
       const size_t c = take_s ? i++ : j++;
-      const size_t a = c * PT, e = std::min(V.size(), a + PT);
+      const size_t a = c * PT, e = std::min(take_s ? SN : FN, a + PT);
       if (panels) plan.h_panels.push_back(PanelD{(uint32_t)plan.h_fast.size(), (uint32_t)(e - a), l, 0});
-      plan.h_fast.insert(plan.h_fast.end(), V.begin() + a, V.begin() + e);
+      for (size_t k = a; k < e; k++)
+        plan.h_fast.push_back(take_s ? sd_task(s_idx[S0 + k]) : fold_task(f_idx[F0 + k]));
     }
   }
   // Units of the warp terminal kernel: maximal runs of tasks on one layout

@@ -178,7 +178,28 @@ struct Ctx {
   StdRng* rng = nullptr;  // the sampled chance mode's generator
 
   const dcfr_menu& menu_for(int street) const { return street == root_street ? *menu : *future; }
-  std::vector<Act> acts(const Betting& st) const { return state_actions(st, menu_for(st.street), bb); }
+  // The action list of a betting state (state_actions), memoised: a tree
+  // repeats the same few hundred states once per dealt card, and the list
+  // depends on nothing else (the menu and big blind are fixed per build).
+  struct StateKey {
+    int64_t v[8];
+    bool operator==(const StateKey& o) const { return std::memcmp(v, o.v, sizeof v) == 0; }
+  };
+  struct StateHash {
+    size_t operator()(const StateKey& k) const {
+      uint64_t h = 1469598103934665603ull;
+      for (int64_t x : k.v) h = (h ^ (uint64_t)x) * 1099511628211ull;
+      return (size_t)h;
+    }
+  };
+  mutable std::unordered_map<StateKey, std::vector<Act>, StateHash> act_cache;
+  const std::vector<Act>& acts(const Betting& st) const {
+    const StateKey k{{(int64_t)st.street | (int64_t)st.to_act << 8 | (int64_t)st.num_raises << 16, st.pot,
+                      st.commit[0], st.commit[1], st.stack[0], st.stack[1], st.current_bet, st.last_raise_inc}};
+    auto it = act_cache.find(k);
+    if (it == act_cache.end()) it = act_cache.emplace(k, state_actions(st, menu_for(st.street), bb)).first;
+    return it->second;
+  }
   float rake(int64_t pot) const {
     return (float)std::min((double)pot * g->cfg.rake_rate, g->cfg.rake_cap);
   }
@@ -242,7 +263,7 @@ static void count_street_over(Ctx& cx, const Betting& st, std::vector<int>& deal
 
 static void count_player(Ctx& cx, const Betting& st, std::vector<int>& dealt, Stats& s) {
   s.player++;
-  auto acts = cx.acts(st);
+  const std::vector<Act>& acts = cx.acts(st);
   s.cells += (uint64_t)acts.size() * (uint64_t)cx.g->n[st.to_act];
   for (const Act& a : acts) {
     Betting s2;
@@ -295,7 +316,7 @@ static void fill_street_over(Ctx& cx, uint32_t id, const Betting& st, int32_t i0
 // Builder::fill_player (tree.rs:451-499).
 static void fill_player(Ctx& cx, uint32_t id, const Betting& st, int32_t i0, int32_t i1, std::vector<int>& dealt) {
   Game& g = *cx.g;
-  auto acts = cx.acts(st);
+  const std::vector<Act>& acts = cx.acts(st);
   uint32_t first = (uint32_t)g.nodes.size();
   g.nodes.resize(g.nodes.size() + acts.size());
   GNode& nd = g.nodes[id];
@@ -638,6 +659,8 @@ int build_game(const dcfr_config& cfg, Game& g, std::string& msg, bool build_tre
     return DCFR_ERR_TOO_LARGE;
   }
   g.nodes.clear();
+  // The count gives the node total: one allocation, no regrowth copies.
+  g.nodes.reserve((size_t)(g.stats.player + g.stats.chance + g.stats.terminal) + 1);
   g.chance.clear();
   g.boards.clear();
   g.storage_len = 0;
