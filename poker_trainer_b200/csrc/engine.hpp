@@ -50,6 +50,9 @@ void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const Te
                             int max_blocks, cudaStream_t s);
 int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
 int panel_terminal_setup(int hpo, int hpp, int cstride, int tstride, int T, int& blocks_per_sm);
+int warp_terminal_dyn_setup(int stride, int cstride, int tstride, int max_warps, int& blocks_per_sm);
+void launch_warp_terminal_dyn(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                              int warps, int max_blocks, uint32_t* counter, cudaStream_t s);
 void launch_panel_terminal(const FastArgs& A, const FastTask* tasks, const PanelD* panels, int npanels, int T, int e,
                            int max_blocks, cudaStream_t s);
 // FP64 best-response oracle kernels (br64.cu).
@@ -262,6 +265,11 @@ class Engine {
   enum TermKernel { TK_PANEL = DCFR_TERMINAL_PANEL, TK_WARP = DCFR_TERMINAL_WARP, TK_BLOCK = DCFR_TERMINAL_BLOCK };
   int term_kernel_ = TK_PANEL;
   int panel_T_ = 0, panel_E_ = 0, panel_blocks_ = 0;
+  // The warp kernel's scheduling: static task ranges per block, or chunks
+  // claimed from term_counter_ (dynamic).
+  bool term_dynamic_ = false;
+  int dyn_warps_ = 0, dyn_blocks_ = 0;
+  uint32_t* term_counter_ = nullptr;
   // Depth-limited solves: the leaf-value network and its buffers.
   dcfr_mlp* net_ = nullptr;
   float* leaf_reach_[2] = {nullptr, nullptr};

@@ -489,6 +489,148 @@ __global__ void __launch_bounds__(512, 1) warp_terminal_kernel(FastArgsT<R> A, c
   }
 }
 
+// The warp-per-terminal evaluation with dynamic scheduling. The static
+// kernel above gives every block an equal share of the task list; the work
+// is not equal (dead subtrees, cfr.rs:267-274, are skipped, and they gather
+// in some parts of the tree as strategies sharpen), so some blocks finish
+// long before others. Here blocks claim chunks of TERM_DYN_CHUNK consecutive
+// tasks from a global counter (zeroed before the launch), stage the layout of
+// each run of the chunk that lies on one layout, and their warps claim the
+// run's tasks one at a time from a shared counter, prefetching the claimed
+// task's row (cp.async) while the current one is evaluated.
+constexpr int TERM_DYN_CHUNK = 128;
+size_t warp_terminal_smem(int stride, int cstride, int tstride, int rsize, int warps);
+
+template <typename R>
+__global__ void __launch_bounds__(512, 1) warp_terminal_dyn_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
+                                                                const TermUnit* __restrict__ units, int nunits,
+                                                                int ntasks, uint32_t* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem_w[];
+  const int W = (int)blockDim.x >> 5;
+  const WarpSmem L_(A.stride, A.cstride, A.tstride, (int)sizeof(R), W);
+  // The chunk's first task and the run's claim counter, after the warps' areas.
+  int& s_base = reinterpret_cast<int*>(smem_w + L_.total)[0];
+  int& s_next = reinterpret_cast<int*>(smem_w + L_.total)[1];
+  uint16_t* ssame = reinterpret_cast<uint16_t*>(smem_w + L_.same);
+  uint16_t* scat = reinterpret_cast<uint16_t*>(smem_w + L_.cat);
+  uint4* srec = reinterpret_cast<uint4*>(smem_w + L_.rec);
+  uint16_t* sseg = reinterpret_cast<uint16_t*>(smem_w + L_.seg);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  R* const row_a = reinterpret_cast<R*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes);
+  R* const row_b = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(row_a) + L_.row_bytes);
+  long long* G = reinterpret_cast<long long*>(smem_w + L_.warp0 + (size_t)warp * L_.warp_bytes + 2 * L_.row_bytes);
+
+  const int p = A.p;
+  const int hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
+  for (int h = tid; h < hpp; h += blockDim.x) {
+    const uint32_t sm = h < np ? A.same[h] : NONE32;
+    ssame[h] = sm == NONE32 ? (uint16_t)0xFFFF : (uint16_t)sm;
+  }
+  uint32_t staged = NONE32;
+  int L = 0;
+  for (;;) {
+    __syncthreads();  // the previous run is finished with the layout and the claim counter
+    if (tid == 0) s_base = (int)atomicAdd(counter, (uint32_t)TERM_DYN_CHUNK);
+    __syncthreads();
+    const int base = s_base;
+    if (base >= ntasks) break;
+    const int end = min(ntasks, base + TERM_DYN_CHUNK);
+    // The unit (maximal run on one layout) holding `base`.
+    int u = 0;
+    {
+      int hi = nunits - 1;
+      while (u < hi) {
+        const int mid = (u + hi) >> 1;
+        if ((int)(units[mid].first + units[mid].count) <= base) u = mid + 1;
+        else hi = mid;
+      }
+    }
+    for (int r0 = base; r0 < end; u++) {
+      const TermUnit U = units[u];
+      const int r1 = min(end, (int)(U.first + U.count));
+      if (U.layout != staged) {  // block-uniform
+        __syncthreads();  // the previous run's warps are done with the layout
+        staged = U.layout;
+        const size_t lay = (size_t)U.layout * 2 + p;
+        const uint16_t* gseg = A.seg + lay * FAST_SEGS;
+        if (tid < FAST_SEGS) sseg[tid] = gseg[tid];
+        L = gseg[FAST_SEGS - 1];
+        const uint16_t* gcat = A.cat + lay * A.cstride;
+        for (int k = tid; k < L; k += blockDim.x) scat[k] = gcat[k];
+        const uint4* grec = A.rec + lay * A.tstride;
+        for (int h = tid; h < np; h += blockDim.x) srec[h] = grec[h];
+      }
+      if (tid == 0) s_next = r0;
+      __syncthreads();  // the layout is staged and the claim counter set
+      const WarpLayout Y{ssame, scat, srec, sseg, L};
+      auto claim = [&]() {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&s_next, 1);
+        return __shfl_sync(0xffffffffu, t, 0);
+      };
+      int cur = claim();
+      bool live = cur < r1 && A.alive[tasks[cur].slot] != 0;
+      if (live) warp_row_prefetch<R>(A, tasks[cur].slot, row_a, lane);
+      cp_async_commit();
+      int buf = 0;
+      while (cur < r1) {
+        const int nxt = claim();
+        const bool nlive = nxt < r1 && A.alive[tasks[nxt].slot] != 0;
+        if (nlive) warp_row_prefetch<R>(A, tasks[nxt].slot, buf ? row_a : row_b, lane);
+        cp_async_commit();
+        cp_async_wait<1>();  // this task's row has landed
+        __syncwarp();
+        // Dead subtree (cfr.rs:267-274): row untouched.
+        if (live) warp_terminal_task<R, true>(A, tasks[cur], Y, buf ? row_b : row_a, G, lane);
+        cur = nxt;
+        live = nlive;
+        buf ^= 1;
+      }
+      cp_async_wait<0>();
+      __syncwarp();
+      r0 = r1;
+      __syncthreads();  // every warp has left this run's claim loop
+    }
+  }
+}
+
+void launch_warp_terminal_dyn(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                              int warps, int max_blocks, uint32_t* counter, cudaStream_t s) {
+  if (nunits <= 0 || ntasks <= 0) return;
+  const int chunks = (ntasks + TERM_DYN_CHUNK - 1) / TERM_DYN_CHUNK;
+  const int blocks = chunks < max_blocks ? chunks : max_blocks;
+  const size_t smem = warp_terminal_smem(A.stride, A.cstride, A.tstride, 4, warps) + 16;
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  warp_terminal_dyn_kernel<float><<<blocks, warps * 32, smem, s>>>(A, tasks, units, nunits, ntasks, counter);
+}
+
+// Warp count (1..max_warps) of the dynamically scheduled kernel that
+// maximises resident warps per SM (its shared memory is the static kernel's
+// plus 16 bytes of counters), and the blocks per SM at that count; 0 if none
+// fits.
+int warp_terminal_dyn_setup(int stride, int cstride, int tstride, int max_warps, int& blocks_per_sm) {
+  int dev = 0, optin = 0;
+  blocks_per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  const void* fn = (const void*)warp_terminal_dyn_kernel<float>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) return 0;
+  int best_w = 0, best_b = 0;
+  for (int w = 1; w <= max_warps; w++) {
+    const size_t smem = warp_terminal_smem(stride, cstride, tstride, 4, w) + 16;
+    if (smem > (size_t)optin) break;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, w * 32, smem) != cudaSuccess) return 0;
+    if (b > 0 && w * b >= best_w * best_b) {
+      best_w = w;
+      best_b = b;
+    }
+  }
+  blocks_per_sm = best_b;
+  return best_w;
+}
+
 size_t warp_terminal_smem(int stride, int cstride, int tstride, int rsize, int warps) {
   return WarpSmem(stride, cstride, tstride, rsize, warps).total;
 }

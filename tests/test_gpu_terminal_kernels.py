@@ -1,8 +1,9 @@
 """The f32 solve's fast-precision terminal kernels against each other.
 
 The panel kernel (terminal_panel.cu: 8 or 4 terminals of one board per
-block pass), the warp-per-terminal kernel and the block-scan kernel
-(terminal_fast.cu, the defaults for short and long hand lists) evaluate the same exact integer prefix sums and
+block pass), the warp-per-terminal kernel with static or dynamic
+scheduling, and the block-scan kernel (terminal_fast.cu; the warp and block
+kernels are the defaults for short and long hand lists) evaluate the same exact integer prefix sums and
 round them with the same f64/f32 operations, so their results must agree
 bit for bit: traversal values from random storage in every mode, and the
 regrets, strategy sums and exploitability after iterations. The kernel is
@@ -18,7 +19,7 @@ from poker_trainer_b200.solver import Solver
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["panel", "panel4", "warp", "block"]
+KERNELS = ["panel", "panel4", "warp", "warpdyn", "block"]
 SPOTS = {
     "river": workloads.river_spot,
     "turn-narrow": workloads.turn_narrow_spot,
@@ -41,7 +42,7 @@ def outputs(make, kernel, monkeypatch):
     monkeypatch.setenv("DCFR_TERMINAL_KERNEL", kernel)
     g = Solver.new(make())
     name, per_panel = g.terminal_kernel()
-    want = "panel" if kernel.startswith("panel") else kernel
+    want = "panel" if kernel.startswith("panel") else "warp" if kernel.startswith("warp") else kernel
     assert name == want, (kernel, name)
     if kernel in ("panel4",):
         assert per_panel == 4
