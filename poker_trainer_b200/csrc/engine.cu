@@ -461,15 +461,17 @@ Status Engine::ensure_fast_layouts() {
   // block) for comparisons.
   const char* sel = std::getenv("DCFR_TERMINAL_KERNEL");
   const std::string want = sel ? sel : (tstride_ <= WARP_TERMINAL_MAX_HANDS ? "warp" : "block");
-  term_kernel_ = want == "warp" || want == "warpdyn" ? TK_WARP : want == "block" ? TK_BLOCK : TK_PANEL;
-  term_dynamic_ = want == "warpdyn";
-  if (term_dynamic_) {
+  term_kernel_ = want == "warp" || want == "warpdyn" ? TK_WARP
+                 : want == "block" || want == "blockdyn" ? TK_BLOCK
+                                                         : TK_PANEL;
+  term_dynamic_ = want == "warpdyn" || want == "blockdyn";
+  if (term_dynamic_ && term_kernel_ == TK_WARP) {
     int bps = 0;
     dyn_warps_ = warp_terminal_dyn_setup(stride_, fcstride_, tstride_, 16, bps);
     dyn_blocks_ = sms * bps;
     if (dyn_warps_ <= 0) term_dynamic_ = false;
-    else if (!(s = dalloc(term_counter_, 1, "terminal counter")).ok()) return s;
   }
+  if (term_dynamic_ && !(s = dalloc(term_counter_, 1, "terminal counter")).ok()) return s;
   if (term_kernel_ == TK_PANEL) {
     const int o0 = 1, o1 = 0;  // opponent of traverser 0 and 1
     panel_T_ = panel_E_ = panel_blocks_ = 0;
@@ -1134,6 +1136,8 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
         launch_warp_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
                              term_warps_[0], term_blocks_[0],
                              stream_);
+      else if (term_dynamic_)
+        launch_fast_terminal_dyn(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, term_counter_, stream_);
       else
         launch_fast_terminal(F, plan.d_fast, (int)plan.h_fast.size(), fast_blocks_, stream_);
     }

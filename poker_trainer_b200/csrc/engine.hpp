@@ -51,6 +51,8 @@ void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const Te
 int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
 int panel_terminal_setup(int hpo, int hpp, int cstride, int tstride, int T, int& blocks_per_sm);
 int warp_terminal_dyn_setup(int stride, int cstride, int tstride, int max_warps, int& blocks_per_sm);
+void launch_fast_terminal_dyn(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, uint32_t* counter,
+                              cudaStream_t s);
 void launch_warp_terminal_dyn(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
                               int warps, int max_blocks, uint32_t* counter, cudaStream_t s);
 void launch_panel_terminal(const FastArgs& A, const FastTask* tasks, const PanelD* panels, int npanels, int T, int e,

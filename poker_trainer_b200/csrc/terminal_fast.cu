@@ -140,9 +140,17 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // stay in registers between the two passes of the scan. R is the row type:
 // float for the solve, double for the FP64 best-response oracle (br64.cu),
 // whose values are formed in double with no rounding to f32.
-template <int E, typename R>
+//
+// DYN: instead of one contiguous range per block, blocks claim chunks of
+// FAST_DYN_CHUNK consecutive tasks from `counter` (zeroed before the launch),
+// so blocks whose tasks are cheap (dead subtrees are skipped) take more.
+// A block claims its next chunk while it starts the current one, so the
+// next task's row can still be prefetched across the chunk boundary.
+constexpr int FAST_DYN_CHUNK = 8;
+
+template <int E, typename R, bool DYN = false>
 __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R> A, const FastTask* __restrict__ tasks,
-                                                                     int ntasks) {
+                                                                     int ntasks, uint32_t* __restrict__ counter = nullptr) {
   extern __shared__ __align__(16) unsigned char smem_fast[];
   constexpr bool F64 = sizeof(R) == 8;
   constexpr int PER16 = 16 / (int)sizeof(R);  // row entries per 16-byte copy
@@ -158,9 +166,20 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
 
   const int p = A.p, o = p ^ 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int hpo = o ? A.hp[1] : A.hp[0], hpp = p ? A.hp[1] : A.hp[0], np = p ? A.n[1] : A.n[0];
-  const int per = (ntasks + gridDim.x - 1) / gridDim.x;
-  const int t0 = blockIdx.x * per, t1 = min(ntasks, t0 + per);
+  __shared__ int s_claim[2];  // DYN: the first chunk, then the chunk after the current one
+  int t0, t1;
+  if constexpr (DYN) {
+    if (tid == 0) s_claim[0] = (int)atomicAdd(counter, (uint32_t)FAST_DYN_CHUNK);
+    __syncthreads();
+    t0 = s_claim[0];
+    t1 = ntasks;
+  } else {
+    const int per = (ntasks + gridDim.x - 1) / gridDim.x;
+    t0 = blockIdx.x * per;
+    t1 = min(ntasks, t0 + per);
+  }
   if (t0 >= t1) return;
+  int cbeg = t0, cend = min(t1, t0 + FAST_DYN_CHUNK), claimed = t1;  // DYN: current chunk, next chunk
 
   for (int h = tid; h < hpp; h += FAST_THREADS) {
     const uint32_t sm = h < np ? A.same[h] : NONE32;
@@ -181,8 +200,12 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
   // scan's warp totals (2) and after the prefixes are written (3). The next
   // terminal's barrier (1) also ends this one's reads of the prefixes, the
   // layout and this row buffer.
-  for (int ti = t0; ti < t1; ti++) {
-    const int buf = (ti - t0) & 1;
+  int step = 0;
+  for (int ti = t0; ti < t1;) {
+    const int buf = step & 1;
+    step++;
+    const bool first = DYN && ti == cbeg;
+    if (first && tid == 0) s_claim[1] = (int)atomicAdd(counter, (uint32_t)FAST_DYN_CHUNK);
     const R* r = rbuf + (size_t)buf * A.stride;
     // Row ti landed (own copies), partial maxima published.
     cp_async_wait_all();
@@ -202,9 +225,23 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
     for (int d = 16; d > 0; d >>= 1) mx = row_max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
     if (lane == 0) fred[buf * (FAST_THREADS / 32) + warp] = mx;
     __syncthreads();  // (1)
-    if (ti + 1 < t1) prefetch(ti + 1, buf ^ 1);
+    // The task after ti: the next in its range, or (DYN) the first of the
+    // chunk claimed while this chunk started.
+    int next;
+    if constexpr (DYN) {
+      if (first) claimed = s_claim[1];
+      next = ti + 1 < cend ? ti + 1 : min(claimed, t1);
+    } else {
+      next = ti + 1;
+    }
+    if (next < t1) prefetch(next, buf ^ 1);
     const FastTask cur = T;
-    if (ti + 1 < t1) T = tasks[ti + 1];  // next task's record, loaded early
+    if (next < t1) T = tasks[next];  // next task's record, loaded early
+    if (DYN && next != ti + 1) {
+      cbeg = next;
+      cend = min(t1, next + FAST_DYN_CHUNK);
+    }
+    ti = next;
     if (A.alive[cur.slot] == 0) continue;  // dead subtree (cfr.rs:267-274): row untouched
     if (cur.board != board) {
       board = cur.board;
@@ -335,6 +372,8 @@ static cudaError_t setup_e(int optin, size_t smem, int& blocks) {
                                        optin);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(fast_terminal_kernel<E, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(fast_terminal_kernel<E, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel<E, float>, FAST_THREADS, smem);
 }
@@ -698,6 +737,23 @@ static void launch_fast_terminal_t(const FastArgsT<R>& A, const FastTask* tasks,
 #define FAST_E(e_)                                                                     \
   case e_:                                                                             \
     fast_terminal_kernel<e_, R><<<blocks, FAST_THREADS, smem, s>>>(A, tasks, ntasks); \
+    break;
+    FAST_E(1) FAST_E(3) FAST_E(5) FAST_E(7) FAST_E(9) FAST_E(11) FAST_E(13) FAST_E(15) FAST_E(17)
+#undef FAST_E
+  }
+}
+
+void launch_fast_terminal_dyn(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, uint32_t* counter,
+                              cudaStream_t s) {
+  if (ntasks <= 0) return;
+  const int chunks = (ntasks + FAST_DYN_CHUNK - 1) / FAST_DYN_CHUNK;
+  const int blocks = chunks < max_blocks ? chunks : max_blocks;
+  const size_t smem = fast_smem_bytes(A.stride, A.emax, A.cstride, A.tstride, 4);
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  switch (A.emax) {
+#define FAST_E(e_)                                                                                        \
+  case e_:                                                                                                \
+    fast_terminal_kernel<e_, float, true><<<blocks, FAST_THREADS, smem, s>>>(A, tasks, ntasks, counter); \
     break;
     FAST_E(1) FAST_E(3) FAST_E(5) FAST_E(7) FAST_E(9) FAST_E(11) FAST_E(13) FAST_E(15) FAST_E(17)
 #undef FAST_E

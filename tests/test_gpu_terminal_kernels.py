@@ -19,7 +19,7 @@ from poker_trainer_b200.solver import Solver
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["panel", "panel4", "warp", "warpdyn", "block"]
+KERNELS = ["panel", "panel4", "warp", "warpdyn", "block", "blockdyn"]
 SPOTS = {
     "river": workloads.river_spot,
     "turn-narrow": workloads.turn_narrow_spot,
@@ -42,7 +42,7 @@ def outputs(make, kernel, monkeypatch):
     monkeypatch.setenv("DCFR_TERMINAL_KERNEL", kernel)
     g = Solver.new(make())
     name, per_panel = g.terminal_kernel()
-    want = "panel" if kernel.startswith("panel") else "warp" if kernel.startswith("warp") else kernel
+    want = "panel" if kernel.startswith("panel") else "warp" if kernel.startswith("warp") else "block"
     assert name == want, (kernel, name)
     if kernel in ("panel4",):
         assert per_panel == 4
