@@ -226,10 +226,9 @@ def ncu_traffic(kernel: str, workload: str):
 
 
 KERNEL_NAMES = {"terminal": "fast_terminal_kernel", "down": "down_kernel", "up": "up_kernel", "other": "other"}
-# The terminal kernel the engine picks by hand count (more than 768 hands:
-# one block-wide scan per terminal; otherwise one warp per terminal).
-TERMINAL_KERNEL = {"turn": "fast_terminal_kernel", "turn-narrow": "warp_terminal_kernel",
-                   "river": "fast_terminal_kernel", "flop": "warp_terminal_kernel"}
+# The CUDA kernel behind each terminal kernel name of dcfr_terminal_kernel.
+TERMINAL_FN = {"panel": "panel_terminal_kernel", "warp": "warp_terminal_kernel", "block": "fast_terminal_kernel",
+               "exact": "terminal_kernel"}
 
 
 def spawn_ranks(n: int) -> int:
@@ -399,6 +398,7 @@ def run_ours(args, world, rank, local):
     expl = g.exploitability()
     pot = float(cfg.root.pot)
     it_bytes = g.iteration_bytes()
+    tkname, _ = g.terminal_kernel()
     g.close()
 
     value = world * K / (ms / 1000.0)
@@ -428,7 +428,7 @@ def run_ours(args, world, rank, local):
     working = it_bytes
     kname = KERNEL_NAMES[dom]
     if dom == "terminal":
-        kname = TERMINAL_KERNEL[args.workload] if args.precision == "fast" else "terminal_kernel"
+        kname = TERMINAL_FN[tkname]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -498,7 +498,7 @@ def run_turn_secondary(args, grp, local):
     return {"workload": WORKLOADS["turn"], "value": grp.world * args.steps / (ms / 1000.0), "unit": UNIT,
             "ms_per_iteration": ms / args.steps,
             "iteration_roofline_frac": it_bytes * args.steps / (ms / 1000.0) / 1e9 / peak,
-            "terminal_kernel": f"{kname}_terminal_kernel", "terminals_per_panel": per_panel,
+            "terminal_kernel": TERMINAL_FN[kname], "terminals_per_panel": per_panel,
             "terminal_gbs": t["bytes"] / (t["ms"] / 1000.0) / 1e9 if t["ms"] > 0 else None,
             "terminal_frac": (t["bytes"] / (t["ms"] / 1000.0) / 1e9 / peak) if t["ms"] > 0 else None,
             "peak_kind": f"of {peak_kind}"}
@@ -572,7 +572,7 @@ def run_flop(args, world, rank, local):
     per_launch_ms = dc["ms"] / max(dc["launches"], 1)
     per_launch_bytes = dc["bytes"] / max(dc["launches"], 1)
     achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
-    kfull = f"{kname}_terminal_kernel" if dom == "terminal" else KERNEL_NAMES[dom]
+    kfull = TERMINAL_FN[kname] if dom == "terminal" else KERNEL_NAMES[dom]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
