@@ -366,14 +366,23 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
   cp_async_wait_all();
 }
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum less the kernel's own static shared memory (the two together may
+// not pass the opt-in maximum).
+static cudaError_t allow_dynamic_smem(const void* fn, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 template <int E>
 static cudaError_t setup_e(int optin, size_t smem, int& blocks) {
-  cudaError_t e = cudaFuncSetAttribute(fast_terminal_kernel<E, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       optin);
+  cudaError_t e = allow_dynamic_smem((const void*)fast_terminal_kernel<E, float>, optin);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(fast_terminal_kernel<E, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  e = allow_dynamic_smem((const void*)fast_terminal_kernel<E, double>, optin);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(fast_terminal_kernel<E, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  e = allow_dynamic_smem((const void*)fast_terminal_kernel<E, float, true>, optin);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fast_terminal_kernel<E, float>, FAST_THREADS, smem);
 }
@@ -654,7 +663,7 @@ int warp_terminal_dyn_setup(int stride, int cstride, int tstride, int max_warps,
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
     return 0;
   const void* fn = (const void*)warp_terminal_dyn_kernel<float>;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) return 0;
+  if (allow_dynamic_smem(fn, optin) != cudaSuccess) return 0;
   int best_w = 0, best_b = 0;
   for (int w = 1; w <= max_warps; w++) {
     const size_t smem = warp_terminal_smem(stride, cstride, tstride, 4, w) + 16;
@@ -683,7 +692,7 @@ int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
     return 0;
   const void* fn = rsize == 8 ? (const void*)warp_terminal_kernel<double> : (const void*)warp_terminal_kernel<float>;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) return 0;
+  if (allow_dynamic_smem(fn, optin) != cudaSuccess) return 0;
   int best_w = 0, best_b = 0;
   for (int w = 1; w <= max_warps; w++) {
     const size_t smem = warp_terminal_smem(stride, cstride, tstride, rsize, w);
