@@ -1,22 +1,29 @@
 #!/usr/bin/env python3
 """DCFR solve benchmark on B200.
 
-Workload (default): the turn subgame Ks7s2dTh, 48 river runouts, pot 20bb,
-stacks 90bb, 33%/75%/all-in bets and one 2.5x raise on turn and river, ranges
-with class weights U[0,1) from seeds 1000/1001 and 51 of the 169 classes
-zeroed, f32 storage, DCFR alpha 1.5 beta 0 gamma 2. A step is one DCFR
-iteration (both traversals); the metric is DCFR iterations per second.
+Workload (default, --workload flop): the flop full tree Ks7s2d, pot 6bb,
+stacks 97bb, 33%/75%/all-in bets and one 3x raise on every street, ranges
+from a 169-class Dirichlet(0.5) thresholded to 68 classes (seeds 2000/2001),
+f32 storage, suit isomorphism, DCFR alpha 1.5 beta 0 gamma 2. The metric is
+the time to 0.5%-of-the-pot exploitability (seconds, lower is better): one
+solve from a fresh solver with exploitability checks on the reference's
+schedule, the final value re-checked by the FP64 best-response oracle. The
+line also carries the turn subgame's DCFR iterations per second.
+--workload turn | turn-narrow | river | batch | learned measure the other
+configurations (iterations or spot-iterations per second).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs as one process per GPU (torchrun): every rank solves its own copy
-of the spot (independent replicas, no collective on the data path); the
-timed region is bracketed by a barrier and a device synchronize on every
-rank, and the job time is the maximum over ranks.
+of the spot (independent replicas, no collective on the data path; the
+batched spots are partitioned across ranks instead); the timed region is
+bracketed by a barrier and a device synchronize on every rank, and the job
+time is the maximum over ranks.
 
 --impl reference times the CPU restatement of the reference's solver (the
 C++ oracle; the Rust reference cannot be built here) on this host's cores, on
-the same workload and metric; under torchrun only rank 0 runs it.
+the same workload and metric (for the flop: one full solve to the target on
+the same check schedule); under torchrun only rank 0 runs it.
 """
 from __future__ import annotations
 
@@ -228,7 +235,7 @@ def ncu_traffic(kernel: str, workload: str):
 KERNEL_NAMES = {"terminal": "fast_terminal_kernel", "down": "down_kernel", "up": "up_kernel", "other": "other"}
 # The CUDA kernel behind each terminal kernel name of dcfr_terminal_kernel.
 TERMINAL_FN = {"panel": "panel_terminal_kernel", "warp": "warp_terminal_kernel", "block": "fast_terminal_kernel",
-               "exact": "terminal_kernel"}
+               "group": "group_terminal_kernel", "exact": "terminal_kernel"}
 
 
 def spawn_ranks(n: int) -> int:

@@ -393,9 +393,16 @@ int dcfr_last_solve_ms(const dcfr_solver* s, double* ms);
 int dcfr_setup_profile_get(const dcfr_solver* s, dcfr_setup_profile* out);
 
 /* Measurement hook, no counterpart in the reference: the terminal kernel
- * this handle's f32 traversals launch (DCFR_TERMINAL_*), and for the panel
- * kernel the terminals evaluated together per panel (0 otherwise). */
-enum { DCFR_TERMINAL_PANEL = 0, DCFR_TERMINAL_WARP = 1, DCFR_TERMINAL_BLOCK = 2, DCFR_TERMINAL_EXACT = 3 };
+ * this handle's f32 traversals launch (DCFR_TERMINAL_*; GROUP: two warps per
+ * terminal), and for the panel kernel the terminals evaluated together per
+ * panel (0 otherwise). */
+enum {
+  DCFR_TERMINAL_PANEL = 0,
+  DCFR_TERMINAL_WARP = 1,
+  DCFR_TERMINAL_BLOCK = 2,
+  DCFR_TERMINAL_EXACT = 3,
+  DCFR_TERMINAL_GROUP = 4
+};
 int dcfr_terminal_kernel(const dcfr_solver* s, int32_t* kernel, int32_t* terminals_per_panel);
 
 /* Measurement hook, no counterpart in the reference: runs `iterations` DCFR

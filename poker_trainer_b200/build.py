@@ -19,7 +19,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdcfr.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "terminal_panel.cu", "engine.cu", "game.cpp", "capi.cpp",
+SOURCES = ["kernels.cu", "terminal.cu", "terminal_fast.cu", "terminal_panel.cu", "terminal_group.cu", "engine.cu", "game.cpp", "capi.cpp",
            "noalloc.cu", "br64.cu", "batch.cu", "mlp.cu", "leaf.cu"]
 HEADERS = ["engine.hpp", "game.hpp", "plan.hpp", "warp_terminal.cuh", "row_items.cuh", "batch.hpp", "gemm_tc.cuh",
            "chance_sample.hpp", os.path.join("..", "..", "include", "dcfr.h")]

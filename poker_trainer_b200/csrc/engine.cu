@@ -420,6 +420,14 @@ Status Engine::init() {
   for (int p = 0; p < 2; p++)
     if (!(s = upload_plan(*full_[p])).ok()) return s;
   phase(setup.plans_ms);
+  // Default f32 terminal kernel: two warps per terminal where every resident
+  // group has a task in both traversals (measured faster there than both the
+  // warp and the block kernel); the warp or block kernel for fewer tasks
+  // (a river subgame's few terminals: each gets a whole block).
+  if (term_group_auto_) {
+    const size_t resident = (size_t)group_groups_ * (size_t)group_blocks_;
+    term_group_ = full_[0]->h_fast.size() >= resident && full_[1]->h_fast.size() >= resident;
+  }
   if (!(s = dalloc(cur_disc_, 1, "discounts")).ok()) return s;
   if (!(s = dalloc(counter_, 1, "counter")).ok()) return s;
   CK(cudaMemsetAsync(counter_, 0, 4, stream_));
@@ -461,7 +469,7 @@ Status Engine::ensure_fast_layouts() {
   // block) for comparisons.
   const char* sel = std::getenv("DCFR_TERMINAL_KERNEL");
   const std::string want = sel ? sel : (tstride_ <= WARP_TERMINAL_MAX_HANDS ? "warp" : "block");
-  term_kernel_ = want == "warp" || want == "warpdyn" ? TK_WARP
+  term_kernel_ = want == "warp" || want == "warpdyn" || want == "group" ? TK_WARP
                  : want == "block" || want == "blockdyn" ? TK_BLOCK
                                                          : TK_PANEL;
   term_dynamic_ = want == "warpdyn" || want == "blockdyn";
@@ -472,6 +480,16 @@ Status Engine::ensure_fast_layouts() {
     if (dyn_warps_ <= 0) term_dynamic_ = false;
   }
   if (term_dynamic_ && !(s = dalloc(term_counter_, 1, "terminal counter")).ok()) return s;
+  // Two warps per terminal (terminal_group.cu): explicitly, or by default
+  // where both traversals have a task for every resident group (decided in
+  // init once the plans are built).
+  {
+    int bps = 0;
+    group_groups_ = group_terminal_setup(stride_, fcstride_, tstride_, bps);
+    group_blocks_ = sms * bps;
+  }
+  term_group_ = want == "group" && group_groups_ > 0;
+  term_group_auto_ = sel == nullptr && group_groups_ > 0;
   if (term_kernel_ == TK_PANEL) {
     const int o0 = 1, o1 = 0;  // opponent of traverser 0 and 1
     panel_T_ = panel_E_ = panel_blocks_ = 0;
@@ -1129,6 +1147,9 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
       if (term_kernel_ == TK_PANEL)
         launch_panel_terminal(F, plan.d_fast, plan.d_panels, (int)plan.h_panels.size(), panel_T_, panel_E_,
                               panel_blocks_, stream_);
+      else if (term_kernel_ == TK_WARP && term_group_)
+        launch_group_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
+                              group_groups_, group_blocks_, stream_);
       else if (term_kernel_ == TK_WARP && term_dynamic_)
         launch_warp_terminal_dyn(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
                                  dyn_warps_, dyn_blocks_, term_counter_, stream_);

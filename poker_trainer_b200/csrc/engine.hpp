@@ -49,6 +49,9 @@ void launch_warp_terminal64(const FastArgs64& A, const FastTask* tasks, const Te
                             int warps,
                             int max_blocks, cudaStream_t s);
 int warp_terminal_setup(int stride, int cstride, int tstride, int rsize, int max_warps, int& blocks_per_sm);
+int group_terminal_setup(int stride, int cstride, int tstride, int& blocks_per_sm);
+void launch_group_terminal(const FastArgs& A, const FastTask* tasks, const TermUnit* units, int nunits, int ntasks,
+                           int groups, int max_blocks, cudaStream_t s);
 int panel_terminal_setup(int hpo, int hpp, int cstride, int tstride, int T, int& blocks_per_sm);
 int warp_terminal_dyn_setup(int stride, int cstride, int tstride, int max_warps, int& blocks_per_sm);
 void launch_fast_terminal_dyn(const FastArgs& A, const FastTask* tasks, int ntasks, int max_blocks, uint32_t* counter,
@@ -202,7 +205,7 @@ class Engine {
   double iteration_bytes() const;
   // The f32 traversals' terminal kernel (DCFR_TERMINAL_*) and panel width.
   void terminal_kernel(int32_t& kernel, int32_t& per_panel) const {
-    kernel = fast_ ? term_kernel_ : DCFR_TERMINAL_EXACT;
+    kernel = !fast_ ? DCFR_TERMINAL_EXACT : term_group_ ? DCFR_TERMINAL_GROUP : term_kernel_;
     per_panel = fast_ && term_kernel_ == TK_PANEL ? panel_T_ : 0;
   }
   int isomorphic_pairs() const;
@@ -271,6 +274,9 @@ class Engine {
   // claimed from term_counter_ (dynamic).
   bool term_dynamic_ = false;
   int dyn_warps_ = 0, dyn_blocks_ = 0;
+  // Short rows: two warps per terminal (terminal_group.cu) instead of one.
+  bool term_group_ = false, term_group_auto_ = false;
+  int group_groups_ = 0, group_blocks_ = 0;
   uint32_t* term_counter_ = nullptr;
   // Depth-limited solves: the leaf-value network and its buffers.
   dcfr_mlp* net_ = nullptr;

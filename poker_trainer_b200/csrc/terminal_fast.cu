@@ -300,10 +300,6 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
     const uint32_t kind = cur.kind;
     const bool fold = kind == T_FOLD_SCALAR || kind == T_FOLD_BATCH;
     const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
-    // Batched showdown with win = -lose and tie = 0: D = W - L per hand, as
-    // in warp_terminal_task (K_c = card c's start prefix + end prefix), sums
-    // modulo 2^64 (|D| <= T0 < 2^62).
-    const bool dform = !F64 && !fold && !scalar && cur.c == 0.0 && cur.a == -cur.b;
 #pragma unroll 2
     for (int h = tid; h < hpp; h += FAST_THREADS) {
       R v = 0, fv = 0;
@@ -316,17 +312,7 @@ __global__ void __launch_bounds__(FAST_THREADS) fast_terminal_kernel(FastArgsT<R
         const uint16_t sm = ssame[h];
         const long long si = sm == 0xFFFF ? 0ll : fixed(r[sm], scale);
         const long long F = T0 - ca.y - cb.y + si;
-        if (dform) {
-          if (q.w >> 16) {
-            typedef unsigned long long u64;
-            const u64 pos = ((u64)G[q.x & 0xFFFF] + (u64)G[q.x >> 16]) +
-                            ((2ull * (u64)ca.x + (u64)ca.y) + (2ull * (u64)cb.x + (u64)cb.y));
-            const u64 neg = ((u64)T0 + (u64)G[q.y & 0xFFFF]) + ((u64)G[q.y >> 16] + (u64)G[q.z & 0xFFFF]) +
-                            (u64)G[q.z >> 16];
-            v = (R)(pa * (double)(long long)(pos - neg));
-          }
-          if (fout) fv = (R)(pd * (double)F);
-        } else if constexpr (F64) {
+        if constexpr (F64) {
           // Double rows: every value in double, no f32 rounding.
           if (fold) {
             v = pa * (double)F;

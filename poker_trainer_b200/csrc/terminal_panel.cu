@@ -265,10 +265,6 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
       const bool scalar = kind == T_FOLD_SCALAR || kind == T_SHOWDOWN_SCALAR;
       const double pa = tk.a * inv, pb = tk.b * inv, pc = tk.c * inv, pd = tk.d * inv;
       const bool tie = tk.c != 0.0;
-      // Batched showdown with win = -lose and tie = 0: D = W - L per hand, as
-      // in warp_terminal_task (card c's start prefix + end prefix in place of
-      // K_c), sums modulo 2^64 (|D| <= T0 < 2^62).
-      const bool dform = !fold && !scalar && !tie && tk.a == -tk.b;
       const long long T0 = st0[t];
       float* out = A.vals + (size_t)tk.row * A.stride;
       float* fout = tk.frow != NONE32 ? A.vals + (size_t)tk.frow * A.stride : nullptr;
@@ -289,18 +285,6 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1)
         if (fold) {
           // eval_fold (eval.rs:40-64) returns zeros on a zero total.
           v = (scalar && T0 == 0) ? 0.0f : (float)(pa * (double)F);
-          return;
-        }
-        if (dform) {
-          if (q.w >> 16) {
-            typedef unsigned long long u64;
-            const u64 pos = ((u64)Gt[(q.x & 0xFFFF) * T] + (u64)Gt[(q.x >> 16) * T]) +
-                            (((u64)ca.x + (u64)ca.y) + ((u64)cb.x + (u64)cb.y));
-            const u64 neg = ((u64)T0 + (u64)Gt[(q.y & 0xFFFF) * T]) +
-                            ((u64)Gt[(q.y >> 16) * T] + (u64)Gt[(q.z & 0xFFFF) * T]) + (u64)Gt[(q.z >> 16) * T];
-            v = (float)(pa * (double)(long long)(pos - neg));
-          }
-          if (fout) fv = (float)(pd * (double)F);
           return;
         }
         if (q.w >> 16) {

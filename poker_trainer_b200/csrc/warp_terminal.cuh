@@ -210,20 +210,11 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
   const long long total = __shfl_sync(0xffffffffu, inc, 31);
   if (lane == 0) G[L] = total;
   __syncwarp();
-  // A batched showdown whose payoffs are win = -lose and tie = 0 (no rake:
-  // both players invested the same) needs only D = W - L per hand:
-  //   D = (Gw + Gs + K_a + K_b) - (T0 + Gaw + Gas + Gbw + Gbs)
-  // with K_c = 2 x (card c's start prefix) + (card c's total), one product
-  // and one rounding, pa x D (pa x W + pb x L up to the double rounding of
-  // the two products). The sums run modulo 2^64: |D| <= T0 < 2^62, so the
-  // wrapped result is exact.
-  const bool dform = !F64 && !scalar && T.c == 0.0 && T.a == -T.b;
-  // Each card's segment start prefix (or K_c) and total, once per task.
+  // Each card's segment start prefix and total, once per task.
   longlong2* cs = reinterpret_cast<longlong2*>(G + ((L + 2) & ~1));
   for (int c = lane; c < 52; c += 32) {
     const long long s0 = G[Y.seg[1 + c]];
-    const long long tot = G[Y.seg[2 + c]] - s0;
-    cs[c] = make_longlong2(dform ? (long long)(2ull * (unsigned long long)s0 + (unsigned long long)tot) : s0, tot);
+    cs[c] = make_longlong2(s0, G[Y.seg[2 + c]] - s0);
   }
   __syncwarp();
   // 3. Values in hand order.
@@ -237,25 +228,8 @@ __device__ __forceinline__ void warp_terminal_task(const FastArgsT<R>& A, const 
       const uint4 q = Y.rec[h];
       const int a = (int)(q.w & 0xFF), b = (int)((q.w >> 8) & 0xFF);
       const longlong2 ca = cs[a], cb = cs[b];
-      // Identical hand (needed by the paired fold and the tie term only).
-      auto same = [&]() -> long long {
-        const uint16_t sm = Y.same[h];
-        return sm == 0xFFFF ? 0ll : fixed(row[sm], scale);
-      };
-      if constexpr (!F64) {
-        if (dform) {
-          if (q.w >> 16) {
-            typedef unsigned long long u64;
-            const u64 pos = ((u64)G[q.x & 0xFFFF] + (u64)G[q.x >> 16]) + ((u64)ca.x + (u64)cb.x);
-            const u64 neg = ((u64)T0 + (u64)G[q.y & 0xFFFF]) + ((u64)G[q.y >> 16] + (u64)G[q.z & 0xFFFF]) +
-                            (u64)G[q.z >> 16];
-            v = (float)(pa * (double)(long long)(pos - neg));
-          }
-          if (fout) fv = (float)(pd * (double)(T0 - ca.y - cb.y + same()));
-          return;
-        }
-      }
-      const long long si = same();
+      const uint16_t sm = Y.same[h];
+      const long long si = sm == 0xFFFF ? 0ll : fixed(row[sm], scale);
       const long long F = T0 - ca.y - cb.y + si;
       if (q.w >> 16) {
         const long long Gw = G[q.x & 0xFFFF], Gs = G[q.x >> 16];

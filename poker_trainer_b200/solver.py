@@ -480,11 +480,12 @@ class Solver:
 
     def terminal_kernel(self) -> tuple:
         """(kernel name, terminals per panel) of this handle's f32 terminal
-        evaluation: "panel", "warp", "block" or "exact"."""
+        evaluation: "panel", "warp", "block", "group" (two warps per
+        terminal) or "exact"."""
         k = C.c_int32()
         t = C.c_int32()
         check(lib().dcfr_terminal_kernel(self._h, C.byref(k), C.byref(t)))
-        return ("panel", "warp", "block", "exact")[k.value], t.value
+        return ("panel", "warp", "block", "exact", "group")[k.value], t.value
 
     def kernel_launches(self) -> int:
         x = C.c_uint64()

@@ -165,3 +165,23 @@ def test_fast_workload_exploitability(gpu, spot):
     g.iterate(iters)
     eo, eg = o.exploitability(), g.exploitability()
     assert abs(eg - eo) <= EXPLOITABILITY_RTOL * abs(eo), (eg, eo)
+
+
+def test_fast_trajectory_tracks_oracle(gpu):
+    """Fast precision rounds each terminal value in the reference's own
+    operation order, so along a solve the exploitability stays equal to the
+    oracle's (up to rare one-rounding-step differences), not merely close:
+    DCFR amplifies any systematic rounding change within tens of iterations
+    (a single-product showdown rounding moved the flop's exploitability by
+    5e-4 relative after 40 iterations). Turn Ks7s2dTh with the flop
+    workload's ranges, checked at 20, 80 and 160 iterations."""
+    cfg = workloads.turn_narrow_spot()
+    o = OracleSolver(cfg)
+    g = Solver.new(cfg)
+    done = 0
+    for mark in (20, 80, 160):
+        o.iterate(mark - done)
+        g.iterate(mark - done)
+        done = mark
+        eo, eg = o.exploitability(), g.exploitability()
+        assert abs(eg - eo) <= 1e-7 * abs(eo), (mark, eg, eo)

@@ -2,8 +2,9 @@
 
 The panel kernel (terminal_panel.cu: 8 or 4 terminals of one board per
 block pass), the warp-per-terminal kernel with static or dynamic
-scheduling, and the block-scan kernel (terminal_fast.cu; the warp and block
-kernels are the defaults for short and long hand lists) evaluate the same exact integer prefix sums and
+scheduling, the two-warps-per-terminal kernel (terminal_group.cu, the default
+where every resident group has a task) and the block-scan kernel
+(terminal_fast.cu) evaluate the same exact integer prefix sums and
 round them with the same f64/f32 operations, so their results must agree
 bit for bit: traversal values from random storage in every mode, and the
 regrets, strategy sums and exploitability after iterations. The kernel is
@@ -19,7 +20,7 @@ from poker_trainer_b200.solver import Solver
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ["panel", "panel4", "warp", "warpdyn", "block", "blockdyn"]
+KERNELS = ["panel", "panel4", "warp", "warpdyn", "group", "block", "blockdyn"]
 SPOTS = {
     "river": workloads.river_spot,
     "turn-narrow": workloads.turn_narrow_spot,
@@ -42,7 +43,8 @@ def outputs(make, kernel, monkeypatch):
     monkeypatch.setenv("DCFR_TERMINAL_KERNEL", kernel)
     g = Solver.new(make())
     name, per_panel = g.terminal_kernel()
-    want = "panel" if kernel.startswith("panel") else "warp" if kernel.startswith("warp") else "block"
+    want = ("panel" if kernel.startswith("panel") else "warp" if kernel.startswith("warp") else "group"
+            if kernel == "group" else "block")
     assert name == want, (kernel, name)
     if kernel in ("panel4",):
         assert per_panel == 4
@@ -82,9 +84,12 @@ def test_terminal_kernels_bit_identical(gpu, name, monkeypatch):
             assert same_bits(got[key], ref[key]), f"{name}: {kernel} differs from warp in {key}"
 
 
-def test_default_kernel_by_hand_count(gpu, monkeypatch):
+def test_default_kernel_by_task_count(gpu, monkeypatch):
+    """Two warps per terminal where every resident group has a task; a river
+    subgame's few terminals take a whole block each (long hand lists)."""
     monkeypatch.delenv("DCFR_TERMINAL_KERNEL", raising=False)
-    for make, want in ((workloads.turn_spot, ("block", 0)), (workloads.turn_narrow_spot, ("warp", 0))):
+    for make, want in ((workloads.turn_spot, ("group", 0)), (workloads.turn_narrow_spot, ("group", 0)),
+                       (workloads.river_spot, ("block", 0))):
         g = Solver.new(make())
         assert g.terminal_kernel() == want
         g.close()
