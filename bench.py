@@ -828,8 +828,8 @@ def run_learned(args, world, rank, local):
                                               workers=args.learned_workers, part=(rank, world))
     torch.cuda.synchronize()
     t_data = grp.reduce(time.perf_counter() - t0, "max")
-    Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(64, seed=5000, target_pct=0.3, max_iterations=400, with_equity=True,
-                                              workers=args.learned_workers)
+    Xh, Yh, Mh, Eh, _ = leafdata.make_dataset(args.learned_heldout, seed=5000, target_pct=0.3, max_iterations=400,
+                                              with_equity=True, workers=args.learned_workers)
     per_hand_mean = None
     curve = []
     net = None
@@ -941,7 +941,7 @@ def run_learned(args, world, rank, local):
                            "depth_limited_flop_strategy_locked_resolve_exploitability_pct_fp64": 100.0 * e_lock / pot,
                            "locked_resolve_iterations": plk.iteration, "locked_resolve_s": t_lock,
                            "turn_resolve_on_path": turn_resolve},
-        "one_time_cost": {"data_seconds": t_data, "train_seconds": t_train,
+        "one_time_cost": {"data_seconds": t_data, "train_seconds": t_train, "heldout_subgames": args.learned_heldout,
                           "subgames": args.learned_samples, "solve_iterations_mean": float(np.mean(iters)),
                           "note": "paid once for every flop of this shape; not part of a solve"},
         "training": {"curve": curve, "heldout_mse_showdown_equity": masked_mse(Eh, Yh, Mh),
@@ -981,6 +981,7 @@ def main():
     ap.add_argument("--learned-sizes", default=None, metavar="N1,N2,...",
                     help="learned: also train on these prefixes of the data (held-out error against size)")
     ap.add_argument("--learned-workers", type=int, default=4, help="learned: host threads solving subgames")
+    ap.add_argument("--learned-heldout", type=int, default=64, help="learned: held-out subgames (seed 5000)")
     ap.add_argument("--batch-tuning", default=None, metavar="WARPS,BLOCKS_PER_SM,ITERS_PER_LAUNCH,LONGEST_FIRST",
                     help="batch: a fixed launch shape instead of the autotuner's")
     ap.add_argument("--lock-iterations", type=int, default=300,
