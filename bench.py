@@ -551,11 +551,13 @@ def run_flop(args, world, rank, local):
     prog = g.solve(SolveOptions(max_iterations=args.max_iterations, target_exploitability_pct=0.5, check_every=10),
                    on_progress=lambda pr: checks.append((pr.iteration, pr.exploitability_pct)) or True)
     solve_launches = g.kernel_launches() - l0
+    t_solved = time.perf_counter()
     if sampler:
         sampler.end()
     d2h_query = flop_paths_summary(g, pot)
     g.synchronize()
     t_e2e = time.perf_counter() - t0
+    t_solve_wall, t_query = t_solved - t0 - t_create, t_e2e - (t_solved - t0)
     solve_s = grp.reduce(g.last_solve_ms() / 1000.0, "max")
     e2e_s = grp.reduce(t_e2e, "max")
     clocks = sampler.close() if sampler else None
@@ -620,7 +622,8 @@ def run_flop(args, world, rank, local):
         "gpu_launches": int(solve_launches),
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": C.sizeof(cfg) / max(iters, 1),
                 "d2h_bytes_per_step": (8.0 * len(checks) + d2h_query) / max(iters, 1),
-                "create_seconds": t_create, "setup_ms": setup,
+                "create_seconds": t_create, "solve_wall_seconds": t_solve_wall, "query_seconds": t_query,
+                "setup_ms": setup,
                 "what": "dcfr_create from the host config + dcfr_solve to the target (each check reads one f64 "
                         "back) + the root's strategy and EVs read back, wall clock, max over ranks; bytes per "
                         "iteration"},
