@@ -1969,6 +1969,35 @@ Status Engine::subtree_values(uint32_t root, int p, const std::vector<float>& op
   return Status();
 }
 
+// The root's children's values for traverser q under the average strategy:
+// at the root the opponent's reach is its range (as walk() gives there), so
+// one traversal of the full plan (the one the solve runs, in average mode)
+// leaves every child's values in its value row, with the same per-node
+// arithmetic as a subtree plan from that child (subtree_values) and without
+// building one plan per child. A terminal child is the exception: evaluated
+// from itself (as the reference's query does) it is the traversal's root and
+// takes the scalar evaluator, while below a river decision in the full tree
+// it takes the batched one (cfr.rs:282-284), so it keeps its own plan.
+Status Engine::root_child_values(int q, const std::vector<float>& opp_reach, std::vector<std::vector<float>>& child) {
+  const GNode& nd = g.nodes[0];
+  for (uint32_t a = 0; a < nd.nchild; a++) child[a].assign(g.n[q], 0.0f);
+  enqueue_traversal(*full_[q], M_AVG, root_rows_ + (size_t)q * stride_, nullptr);
+  launches += full_[q]->kernels;
+  CK(cudaGetLastError());
+  for (uint32_t a = 0; a < nd.nchild; a++)
+    CK(cudaMemcpyAsync(child[a].data(), vals_ + (size_t)(nd.first + a) * stride_, (size_t)g.n[q] * 4,
+                       cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  for (uint32_t a = 0; a < nd.nchild; a++) {
+    const int kind = g.nodes[nd.first + a].kind;
+    if (kind == N_FOLD || kind == N_SHOWDOWN) {
+      Status s = subtree_values(nd.first + a, q, opp_reach, child[a]);
+      if (!s.ok()) return s;
+    }
+  }
+  return Status();
+}
+
 // query (lib.rs:842-899).
 Status Engine::query(const std::vector<dcfr_step>& path, dcfr_node_info& info, std::vector<Act>& actions,
                      std::vector<uint16_t>& combos, std::vector<float>& strategy, std::vector<float>& ev,
@@ -2000,8 +2029,12 @@ Status Engine::query(const std::vector<dcfr_step>& path, dcfr_node_info& info, s
     }
   }
   std::vector<std::vector<float>> child(na);
-  for (int a = 0; a < na; a++)
-    if (!(s = subtree_values(nd.first + a, q, reach[o], child[a])).ok()) return s;
+  if (node == 0) {
+    if (!(s = root_child_values(q, reach[o], child)).ok()) return s;
+  } else {
+    for (int a = 0; a < na; a++)
+      if (!(s = subtree_values(nd.first + a, q, reach[o], child[a])).ok()) return s;
+  }
   const double offset = g.half_pot + (double)nd.invest[q];
   std::vector<float> strat_c;
   if (!(s = avg_strategy(node, strat_c)).ok()) return s;

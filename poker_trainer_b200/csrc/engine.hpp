@@ -336,6 +336,7 @@ class Engine {
               std::vector<uint32_t> to_canon[2]);
   Status avg_strategy(uint32_t node, std::vector<float>& s);
   Status subtree_values(uint32_t root, int p, const std::vector<float>& opp_reach, std::vector<float>& out);
+  Status root_child_values(int q, const std::vector<float>& opp_reach, std::vector<std::vector<float>>& child);
 };
 
 Status cuda_status(cudaError_t e, const char* what);
