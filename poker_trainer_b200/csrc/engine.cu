@@ -959,6 +959,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   kernels += seg_down_launches + seg_up_launches;
   const int term_kernels = fast_ ? (plan.h_fast.empty() ? 0 : 1) : (int)plan.waves.size();
   kernels += term_kernels;
+  kernels += 1;  // the traversal's start (liveness flags, root row)
   plan.kernels = kernels;
   // Per class: launches and compulsory bytes of one CFR traversal (rows of
   // n floats, f32 storage).
@@ -971,6 +972,7 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   plan.class_kernels[DCFR_KERNEL_DOWN] += tree_launches + seg_down_launches;
   plan.class_kernels[DCFR_KERNEL_UP] += tree_launches + seg_up_launches;
   plan.class_kernels[DCFR_KERNEL_TERMINAL] = term_kernels;
+  plan.class_kernels[DCFR_KERNEL_OTHER] = 1;
   const double np_ = g.n[p], no_ = g.n[o];
   for (const std::vector<DownTask>* v : {&plan.h_down, &plan.h_fdown})
     for (const DownTask& t : *v)
@@ -1116,9 +1118,7 @@ void Engine::fast_args(int p, FastArgs& A) const {
 // up levels (deepest first); the root's value row is copied to root_out.
 void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out) {
   const int p = plan.p, o = p ^ 1;
-  cudaMemsetAsync(alive_, 0, (size_t)plan.nslots * 4, stream_);
-  cudaMemsetAsync(alive_, 1, 4, stream_);
-  cudaMemcpyAsync(reach_, root_row, (size_t)stride_ * 4, cudaMemcpyDeviceToDevice, stream_);
+  launch_traversal_start(alive_, (int)plan.nslots, reach_, root_row, stride_, stream_);
   mark(DCFR_KERNEL_OTHER);
   RowArgs A;
   row_args(p, A);

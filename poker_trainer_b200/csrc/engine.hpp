@@ -71,6 +71,8 @@ int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride);
 void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
 void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
 void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
+void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
+                            cudaStream_t s);
 
 // Status of a failed call: code + message.
 struct Status {

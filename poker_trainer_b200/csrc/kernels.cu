@@ -398,4 +398,38 @@ void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_le
   advance_kernel<<<1, 1, 0, s>>>(counter, table, table_len, cur);
 }
 
+// Start of a traversal: every liveness flag cleared but the root slot's, and
+// the root's reach row copied into slot 0. One launch in place of two
+// memsets and a copy, chained to the traversal's level launches by
+// programmatic dependent launch (the flags are cleared only once the
+// previous traversal's kernels, which read them, are complete).
+__global__ void traversal_start_kernel(uint32_t* __restrict__ alive, int nslots, float* __restrict__ reach,
+                                       const float* __restrict__ root_row, int stride) {
+  pdl_wait();
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x, step = gridDim.x * blockDim.x;
+  for (int i = i0; i < nslots; i += step) alive[i] = i == 0 ? 1u : 0u;
+  for (int i = i0; i < stride / 4; i += step)
+    reinterpret_cast<float4*>(reach)[i] = reinterpret_cast<const float4*>(root_row)[i];
+  pdl_launch_dependents();
+}
+
+void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
+                            cudaStream_t s) {
+  const int threads = 256, work = nslots > stride / 4 ? nslots : stride / 4;
+  int blocks = (work + threads - 1) / threads;
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) blocks = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, traversal_start_kernel, alive, nslots, reach, root_row, stride);
+}
+
 }  // namespace dcfr
