@@ -420,13 +420,14 @@ Status Engine::init() {
   for (int p = 0; p < 2; p++)
     if (!(s = upload_plan(*full_[p])).ok()) return s;
   phase(setup.plans_ms);
-  // Default f32 terminal kernel: two warps per terminal where every resident
-  // group has a task in both traversals (measured faster there than both the
-  // warp and the block kernel); the warp or block kernel for fewer tasks
-  // (a river subgame's few terminals: each gets a whole block).
+  // Default f32 terminal kernel: two warps per terminal where both
+  // traversals have at least four terminal tasks per SM (measured faster there
+  // than both the warp and the block kernel); the warp or block kernel for
+  // fewer tasks (a river subgame's few dozen terminals: each gets a whole
+  // block). The rule depends on the plans and the SM count only.
   if (term_group_auto_) {
-    const size_t resident = (size_t)group_groups_ * (size_t)group_blocks_;
-    term_group_ = full_[0]->h_fast.size() >= resident && full_[1]->h_fast.size() >= resident;
+    const size_t enough = (size_t)4 * (size_t)term_sms_;
+    term_group_ = full_[0]->h_fast.size() >= enough && full_[1]->h_fast.size() >= enough;
   }
   if (!(s = dalloc(cur_disc_, 1, "discounts")).ok()) return s;
   if (!(s = dalloc(counter_, 1, "counter")).ok()) return s;
@@ -481,8 +482,9 @@ Status Engine::ensure_fast_layouts() {
   }
   if (term_dynamic_ && !(s = dalloc(term_counter_, 1, "terminal counter")).ok()) return s;
   // Two warps per terminal (terminal_group.cu): explicitly, or by default
-  // where both traversals have a task for every resident group (decided in
-  // init once the plans are built).
+  // where both traversals have enough terminal tasks (decided in init once
+  // the plans are built).
+  term_sms_ = sms;
   {
     int bps = 0;
     group_groups_ = group_terminal_setup(stride_, fcstride_, tstride_, bps);
@@ -1144,12 +1146,14 @@ void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row
       // Panels of T terminals per block; or (a selectable alternative) a
       // warp per terminal for short rows and one block-wide scan per
       // terminal for long rows.
-      if (term_kernel_ == TK_PANEL)
-        launch_panel_terminal(F, plan.d_fast, plan.d_panels, (int)plan.h_panels.size(), panel_T_, panel_E_,
-                              panel_blocks_, stream_);
-      else if (term_kernel_ == TK_WARP && term_group_)
+      // Two warps per terminal (the default where there are enough tasks,
+      // for short and long hand lists alike) comes first.
+      if (term_group_)
         launch_group_terminal(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
                               group_groups_, group_blocks_, stream_);
+      else if (term_kernel_ == TK_PANEL)
+        launch_panel_terminal(F, plan.d_fast, plan.d_panels, (int)plan.h_panels.size(), panel_T_, panel_E_,
+                              panel_blocks_, stream_);
       else if (term_kernel_ == TK_WARP && term_dynamic_)
         launch_warp_terminal_dyn(F, plan.d_fast, plan.d_units, (int)plan.h_units.size(), (int)plan.h_fast.size(),
                                  dyn_warps_, dyn_blocks_, term_counter_, stream_);

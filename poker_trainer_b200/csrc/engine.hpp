@@ -278,7 +278,7 @@ class Engine {
   int dyn_warps_ = 0, dyn_blocks_ = 0;
   // Short rows: two warps per terminal (terminal_group.cu) instead of one.
   bool term_group_ = false, term_group_auto_ = false;
-  int group_groups_ = 0, group_blocks_ = 0;
+  int group_groups_ = 0, group_blocks_ = 0, term_sms_ = 0;
   uint32_t* term_counter_ = nullptr;
   // Depth-limited solves: the leaf-value network and its buffers.
   dcfr_mlp* net_ = nullptr;

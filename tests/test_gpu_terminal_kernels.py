@@ -3,7 +3,8 @@
 The panel kernel (terminal_panel.cu: 8 or 4 terminals of one board per
 block pass), the warp-per-terminal kernel with static or dynamic
 scheduling, the two-warps-per-terminal kernel (terminal_group.cu, the default
-where every resident group has a task) and the block-scan kernel
+where both traversals have at least four terminal tasks per SM) and the
+block-scan kernel
 (terminal_fast.cu) evaluate the same exact integer prefix sums and
 round them with the same f64/f32 operations, so their results must agree
 bit for bit: traversal values from random storage in every mode, and the
@@ -85,8 +86,9 @@ def test_terminal_kernels_bit_identical(gpu, name, monkeypatch):
 
 
 def test_default_kernel_by_task_count(gpu, monkeypatch):
-    """Two warps per terminal where every resident group has a task; a river
-    subgame's few terminals take a whole block each (long hand lists)."""
+    """Two warps per terminal where both traversals have at least four
+    terminal tasks per SM; a river subgame's few dozen terminals take a whole
+    block each (long hand lists)."""
     monkeypatch.delenv("DCFR_TERMINAL_KERNEL", raising=False)
     for make, want in ((workloads.turn_spot, ("group", 0)), (workloads.turn_narrow_spot, ("group", 0)),
                        (workloads.river_spot, ("block", 0))):
