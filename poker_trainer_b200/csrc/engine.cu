@@ -8,7 +8,6 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
-#include <deque>
 #include <thread>
 #include <unordered_map>
 
@@ -198,6 +197,7 @@ Engine::~Engine() {
   }
   dfree(leaf_x_);
   dfree(leaf_cards_);
+  dfree(sblk_);
   dfree(reach64_);
   dfree(vals64_);
   dfree(root_rows64_);
@@ -539,13 +539,15 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   std::vector<SdLane> sd;
   std::vector<TermLane> folds[2];
   uint32_t next_slot = 1;
-  std::deque<std::pair<uint32_t, uint32_t>> q;  // node, depth
-  std::vector<uint32_t> slot_of;                // by BFS discovery, indexed via map below
-  std::vector<uint32_t> node_slot;
-  // Per-node scratch, dense over node ids (a subtree plan touches a part).
+  // Breadth-first queue (popped at qh). An entry carries what the node
+  // inherits from its parent: its reach slot, chance layer, and the parent's
+  // fused segment, depth in it and depth in a wide segment (NONE32: none).
+  struct QItem {
+    uint32_t v, depth, slot, layer, ptree, ptdepth, psdepth;
+  };
+  std::vector<QItem> q;
+  size_t qh = 0;
   const size_t NN = g.nodes.size();
-  std::vector<uint32_t> slot(NN, 0);
-  slot[root] = 0;
   // Every street's decision subtree is a segment: the traversal's root and
   // each child of a chance node. A segment runs fused (one block,
   // fused_*_kernel) or level by level. Chance nodes sit between segments;
@@ -561,82 +563,125 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // segment, wide segments) run level by level: one launch per depth, with
   // many blocks per node.
   constexpr uint32_t FUSE_MAX_NODES = 48, FUSE_MIN_SEGMENTS = 16;
+  // The traversal's nodes in id order. build_game appends a node's children
+  // after it, so ids grow from parent to child and a pass in id order visits
+  // every parent before its children (the reverse pass, children first).
+  std::vector<uint32_t> sub;
+  if (root == 0) {
+    sub.resize(NN);
+    for (uint32_t v = 0; v < NN; v++) sub[v] = v;
+  } else {
+    std::vector<uint32_t> st{root};
+    while (!st.empty()) {
+      const uint32_t v = st.back();
+      st.pop_back();
+      sub.push_back(v);
+      const GNode& nd = g.nodes[v];
+      if (nd.kind == N_PLAYER || nd.kind == N_CHANCE)
+        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back(nd.first + i);
+    }
+    std::sort(sub.begin(), sub.end());
+  }
+  // Decision nodes per segment (keyed by the segment's root) and segments
+  // per chance layer.
   std::vector<uint32_t> seg_size(NN, 0);
   std::vector<uint32_t> layer_segments;
+  size_t nplayer = 0, nshow = 0, nfold = 0;  // the traversal's nodes by kind (capacities)
   {
-    struct Item {
-      uint32_t v, seg, layer;
-    };
-    std::vector<Item> st{{root, root, 0}};
-    while (!st.empty()) {
-      const Item it = st.back();
-      st.pop_back();
-      const GNode& nd = g.nodes[it.v];
-      if (nd.kind == N_PLAYER) {
-        uint32_t rr = it.seg;
-        if (segment_root(it.v)) {
-          rr = it.v;
-          if (layer_segments.size() <= it.layer) layer_segments.resize(it.layer + 1, 0);
-          layer_segments[it.layer]++;
+    std::vector<uint32_t> seg_of(NN, 0), lay(NN, 0);
+    for (const uint32_t v : sub) {
+      const GNode& nd = g.nodes[v];
+      uint32_t seg = root, layer = 0;
+      if (v != root) {
+        const uint32_t u = nd.parent;
+        if (g.nodes[u].kind == N_PLAYER) {
+          seg = seg_of[u];
+          layer = lay[u];
+        } else {
+          seg = v;
+          layer = lay[u] + 1;
         }
-        seg_size[rr]++;
-        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back({nd.first + i, rr, it.layer});
-      } else if (nd.kind == N_CHANCE) {
-        for (uint32_t i = 0; i < nd.nchild; i++) st.push_back({nd.first + i, nd.first + i, it.layer + 1});
       }
+      lay[v] = layer;
+      nshow += nd.kind == N_SHOWDOWN;
+      nfold += nd.kind == N_FOLD;
+      if (nd.kind != N_PLAYER) continue;
+      nplayer++;
+      uint32_t rr = seg;
+      if (segment_root(v)) {
+        rr = v;
+        if (layer_segments.size() <= layer) layer_segments.resize(layer + 1, 0);
+        layer_segments[layer]++;
+      }
+      seg_size[rr]++;
+      seg_of[v] = rr;
     }
   }
   auto fused_segment = [&](uint32_t v, uint32_t layer) {
     return seg_size[v] <= FUSE_MAX_NODES && layer < layer_segments.size() &&
            layer_segments[layer] >= FUSE_MIN_SEGMENTS;
   };
-  std::vector<uint32_t> tree_id(NN, NONE32), tree_depth(NN, 0);  // node -> fused tree and depth in it
-  std::vector<uint32_t> layer_of(NN, 0), sdepth_of(NN, NONE32);  // chance layer; depth in a wide segment
-  std::vector<std::vector<std::vector<DownTask>>> sdown;                // wide segments: [layer][depth]
+  std::vector<std::vector<std::vector<DownTask>>> sdown;  // wide segments: [layer][depth]
   std::vector<std::vector<std::vector<UpTask>>> sup;
-  layer_of[root] = 0;
-  std::vector<std::vector<std::pair<uint32_t, DownTask>>> fdown;
-  std::vector<std::vector<std::pair<uint32_t, UpTask>>> fup;
+  // Fused segments' tasks in discovery (breadth-first) order with their
+  // segment and depth in it; bucketed by segment below.
+  struct FDown {
+    uint32_t tree, depth;
+    DownTask t;
+  };
+  struct FUp {
+    uint32_t tree, depth;
+    UpTask t;
+  };
+  std::vector<FDown> fdown;
+  std::vector<FUp> fup;
   std::vector<uint32_t> tree_layer;
   int fmaxa = 0;
-  q.push_back({root, 0});
+  q.reserve(sub.size());
+  fdown.reserve(nplayer);
+  fup.reserve(nplayer);
+  sd.reserve(nshow);
+  folds[1].reserve(nfold);
+  q.push_back({root, 0, 0, 0, NONE32, 0, NONE32});
   const double hp = g.half_pot, norm = g.norm;
   uint64_t count = 0;
-  while (!q.empty()) {
-    auto [v, depth] = q.front();
-    q.pop_front();
+  while (qh < q.size()) {
+    // The queue holds the next nodes already: request their records ahead
+    // of use (breadth-first order jumps across the node array).
+    if (qh + 24 < q.size()) {
+      const uint32_t w = q[qh + 24].v;
+      __builtin_prefetch(&g.nodes[w]);
+      __builtin_prefetch(&gpu_off_[w]);
+      __builtin_prefetch(&seg_size[w]);
+    }
+    if (qh + 8 < q.size()) {
+      const GNode& wn = g.nodes[q[qh + 8].v];
+      if (wn.kind == N_PLAYER || wn.kind == N_CHANCE) __builtin_prefetch(&g.nodes[wn.first]);
+    }
+    const QItem it = q[qh++];
+    const uint32_t v = it.v, depth = it.depth;
     count++;
     const GNode& nd = g.nodes[v];
-    const uint32_t sv = slot[v];
-    const uint32_t layer = layer_of[v];
-    if (nd.kind == N_PLAYER || nd.kind == N_CHANCE)
-      for (uint32_t i = 0; i < nd.nchild; i++) layer_of[nd.first + i] = layer + (nd.kind == N_CHANCE ? 1u : 0u);
-    uint32_t tree = NONE32, tdepth = 0;
+    const uint32_t sv = it.slot;
+    const uint32_t layer = it.layer;
+    const uint32_t clayer = layer + (nd.kind == N_CHANCE ? 1u : 0u);  // the children's
+    uint32_t tree = NONE32, tdepth = 0, sdepth = NONE32;
     if (segment_root(v) && fused_segment(v, layer)) {
-      tree = (uint32_t)fdown.size();
-      fdown.emplace_back();
-      fup.emplace_back();
+      tree = (uint32_t)tree_layer.size();
       tree_layer.push_back(layer);
     } else if (segment_root(v)) {
-      sdepth_of[v] = 0;
-    } else if (nd.kind == N_PLAYER && nd.parent != NO && tree_id[nd.parent] != NONE32) {
-      tree = tree_id[nd.parent];
-      tdepth = tree_depth[nd.parent] + 1;
-    }
-    if (tree != NONE32) {
-      tree_id[v] = tree;
-      tree_depth[v] = tdepth;
+      sdepth = 0;
+    } else if (nd.kind == N_PLAYER && it.ptree != NONE32) {
+      tree = it.ptree;
+      tdepth = it.ptdepth + 1;
     }
     if (tree != NONE32 && nd.kind == N_PLAYER) {
       // Inside a fused river subtree (no chance nodes below the river).
       bool own = nd.player == p;
       uint32_t first_slot = own ? sv : next_slot;
       if (!own) next_slot += nd.nchild;
-      for (uint32_t i = 0; i < nd.nchild; i++) {
-        uint32_t c = nd.first + i;
-        slot[c] = own ? sv : first_slot + i;
-        q.push_back({c, depth + 1});
-      }
+      for (uint32_t i = 0; i < nd.nchild; i++)
+        q.push_back({nd.first + i, depth + 1, own ? sv : first_slot + i, clayer, tree, tdepth, NONE32});
       if (nd.nchild > MAX_ACTIONS) {
         Status s;
         s.code = DCFR_ERR_INVALID_ARG;
@@ -645,8 +690,8 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       }
       // `cards` of a decision node's tasks: its scale slot (compressed storage).
       if (!own)
-        fdown[tree].push_back({tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], nd.index, 0.0f}});
-      fup[tree].push_back({tdepth, UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
+        fdown.push_back({tree, tdepth, DownTask{D_OPP_SPLIT, sv, first_slot, nd.nchild, gpu_off_[v], nd.index, 0.0f}});
+      fup.push_back({tree, tdepth, UpTask{own ? (uint32_t)U_OWN : (uint32_t)U_OPP_SUM, sv, v, nd.first, nd.nchild,
                                           first_slot, gpu_off_[v], nd.index, 0, 0, 0}});
       fmaxa = std::max<int>(fmaxa, (int)nd.nchild);
     } else if (nd.kind == N_PLAYER || nd.kind == N_CHANCE) {
@@ -667,15 +712,12 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
       bool own = nd.kind == N_PLAYER && nd.player == p;
       uint32_t first_slot = own ? sv : next_slot;
       if (!own) next_slot += nd.nchild;
-      for (uint32_t i = 0; i < nd.nchild; i++) {
-        uint32_t c = nd.first + i;
-        slot[c] = own ? sv : first_slot + i;
-        q.push_back({c, depth + 1});
-      }
+      if (nd.kind == N_PLAYER && sdepth == NONE32) sdepth = it.psdepth + 1;
+      for (uint32_t i = 0; i < nd.nchild; i++)
+        q.push_back({nd.first + i, depth + 1, own ? sv : first_slot + i, clayer, tree, tdepth, sdepth});
       if (nd.kind == N_PLAYER) {
         // A node of a wide segment: level by level.
-        if (sdepth_of[v] == NONE32) sdepth_of[v] = sdepth_of[nd.parent] + 1;
-        const uint32_t sd = sdepth_of[v];
+        const uint32_t sd = sdepth;
         if (sdown.size() <= layer) {
           sdown.resize(layer + 1);
           sup.resize(layer + 1);
@@ -753,9 +795,28 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   plan.h_fup.clear();
   plan.fused_maxa = fmaxa;
   // Segments by layer: one fused launch per layer.
-  std::vector<uint32_t> order(fdown.size());
+  const uint32_t ntrees = (uint32_t)tree_layer.size();
+  std::vector<uint32_t> order(ntrees);
   for (size_t t = 0; t < order.size(); t++) order[t] = (uint32_t)t;
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return tree_layer[a] < tree_layer[b]; });
+  // Each segment's tasks, discovery order kept (counting sort by segment).
+  std::vector<uint32_t> fd_off(ntrees + 1, 0), fu_off(ntrees + 1, 0);
+  for (const FDown& x : fdown) fd_off[x.tree + 1]++;
+  for (const FUp& x : fup) fu_off[x.tree + 1]++;
+  for (uint32_t t = 0; t < ntrees; t++) {
+    fd_off[t + 1] += fd_off[t];
+    fu_off[t + 1] += fu_off[t];
+  }
+  std::vector<uint32_t> fd_idx(fdown.size()), fu_idx(fup.size());
+  {
+    std::vector<uint32_t> fill(fd_off.begin(), fd_off.end() - 1);
+    for (size_t i = 0; i < fdown.size(); i++) fd_idx[fill[fdown[i].tree]++] = (uint32_t)i;
+    std::vector<uint32_t> ufill(fu_off.begin(), fu_off.end() - 1);
+    for (size_t i = 0; i < fup.size(); i++) fu_idx[ufill[fup[i].tree]++] = (uint32_t)i;
+  }
+  plan.h_fdown.reserve(fdown.size());
+  plan.h_fup.reserve(fup.size());
+  plan.h_trees.reserve(ntrees);
   plan.tree_layers.clear();
   for (uint32_t t : order) {
     const uint32_t l = tree_layer[t];
@@ -763,17 +824,23 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
     plan.tree_layers[l].second++;
     FusedTree F{(uint32_t)plan.h_fdown.size(), 0, (uint32_t)plan.h_fup.size(), 0};
     uint32_t prev = 0;
-    for (size_t i = 0; i < fdown[t].size(); i++) {
-      DownTask T = fdown[t][i].second;
-      if (i > 0 && fdown[t][i].first != prev) T.kind |= LEVEL_BREAK;
-      prev = fdown[t][i].first;
+    for (uint32_t i = fd_off[t]; i < fd_off[t + 1]; i++) {
+      const FDown& x = fdown[fd_idx[i]];
+      DownTask T = x.t;
+      if (i > fd_off[t] && x.depth != prev) T.kind |= LEVEL_BREAK;
+      prev = x.depth;
       plan.h_fdown.push_back(T);
     }
-    std::stable_sort(fup[t].begin(), fup[t].end(),
-                     [](const std::pair<uint32_t, UpTask>& a, const std::pair<uint32_t, UpTask>& b) {
-                       return a.first > b.first;
-                     });
-    for (auto& x : fup[t]) plan.h_fup.push_back(x.second);
+    // Up tasks deepest level first, discovery order within a level: the
+    // segment's levels (depth non-decreasing in discovery order) reversed.
+    uint32_t e = fu_off[t + 1];
+    while (e > fu_off[t]) {
+      uint32_t b = e - 1;
+      const uint32_t d = fup[fu_idx[b]].depth;
+      while (b > fu_off[t] && fup[fu_idx[b - 1]].depth == d) b--;
+      for (uint32_t i = b; i < e; i++) plan.h_fup.push_back(fup[fu_idx[i]].t);
+      e = b;
+    }
     F.down_count = (uint32_t)(plan.h_fdown.size() - F.down_first);
     F.up_count = (uint32_t)(plan.h_fup.size() - F.up_first);
     plan.h_trees.push_back(F);
@@ -842,12 +909,22 @@ Status Engine::build_plan(uint32_t root, int p, Plan& plan) {
   // the terminal kernels take contiguous task ranges; folds are cheaper).
   // Other folds use the fold layout (index nboards).
   const uint32_t nb = (uint32_t)g.boards.size();
-  std::vector<uint32_t> seg_board(NN, NONE32);  // decision node -> river board below it
-  for (const SdLane& x : sd) {
-    uint32_t u = g.nodes[x.lane.row].parent;
-    while (u != NO && g.nodes[u].kind == N_PLAYER && seg_board[u] == NONE32) {
-      seg_board[u] = x.board;
-      u = g.nodes[u].parent;
+  // Decision node -> the river board below it: passed up from each showdown
+  // through its decision-node ancestors (one street segment; every showdown
+  // below a decision node of that segment has the same board), children
+  // first, then above the traversal's root.
+  std::vector<uint32_t> seg_board(NN, NONE32);
+  for (size_t i = sub.size(); i-- > 0;) {
+    const uint32_t v = sub[i];
+    const GNode& nd = g.nodes[v];
+    const uint32_t b = nd.kind == N_SHOWDOWN ? nd.index : nd.kind == N_PLAYER ? seg_board[v] : NONE32;
+    if (b == NONE32 || nd.parent == NO) continue;
+    if (v == root) {
+      for (uint32_t u = nd.parent; u != NO && g.nodes[u].kind == N_PLAYER && seg_board[u] == NONE32;
+           u = g.nodes[u].parent)
+        seg_board[u] = b;
+    } else if (g.nodes[nd.parent].kind == N_PLAYER && seg_board[nd.parent] == NONE32) {
+      seg_board[nd.parent] = b;
     }
   }
   // Each fold's layout, then per layout the showdowns' and folds' indices
@@ -1706,28 +1783,29 @@ Status Engine::solve_loop(const dcfr_solve_options& opts, const volatile int32_t
 }
 
 Status Engine::download(float* regrets, float* sums) {
+  if (!compressed_) {
+    // Packed on the device and copied straight into the caller's arrays.
+    Status s;
+    if (regrets && !(s = storage_out(regrets_, regrets, 4)).ok()) return s;
+    if (sums && !(s = storage_out(sums_, sums, 4)).ok()) return s;
+    return Status();
+  }
+  // Decoded as load_regrets / load_strat do (storage.rs:226-268).
   std::vector<float> r(gpu_len_), sm(gpu_len_);
-  if (compressed_) {
-    // Decoded as load_regrets / load_strat do (storage.rs:226-268).
-    std::vector<int16_t> rq(gpu_len_);
-    std::vector<uint16_t> sq(gpu_len_);
-    std::vector<float> rs, ss;
-    Status s = download_compressed_raw(rq, sq, rs, ss);
-    if (!s.ok()) return s;
-    for (uint32_t v = 0; v < g.nodes.size(); v++) {
-      const GNode& nd = g.nodes[v];
-      if (nd.kind != N_PLAYER) continue;
-      const size_t len = (size_t)nd.nchild * hp_[nd.player];
-      const float rsc = rs[nd.index] / 32767.0f, ssc = ss[nd.index] / 65535.0f;
-      for (size_t i = 0; i < len; i++) {
-        r[gpu_off_[v] + i] = (float)rq[gpu_off_[v] + i] * rsc;
-        sm[gpu_off_[v] + i] = (float)sq[gpu_off_[v] + i] * ssc;
-      }
+  std::vector<int16_t> rq(gpu_len_);
+  std::vector<uint16_t> sq(gpu_len_);
+  std::vector<float> rs, ss;
+  Status s = download_compressed_raw(rq, sq, rs, ss);
+  if (!s.ok()) return s;
+  for (uint32_t v = 0; v < g.nodes.size(); v++) {
+    const GNode& nd = g.nodes[v];
+    if (nd.kind != N_PLAYER) continue;
+    const size_t len = (size_t)nd.nchild * hp_[nd.player];
+    const float rsc = rs[nd.index] / 32767.0f, ssc = ss[nd.index] / 65535.0f;
+    for (size_t i = 0; i < len; i++) {
+      r[gpu_off_[v] + i] = (float)rq[gpu_off_[v] + i] * rsc;
+      sm[gpu_off_[v] + i] = (float)sq[gpu_off_[v] + i] * ssc;
     }
-  } else {
-    CK(cudaMemcpyAsync(r.data(), regrets_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(sm.data(), sums_, gpu_len_ * 4, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
   }
   for (uint32_t v = 0; v < g.nodes.size(); v++) {
     const GNode& nd = g.nodes[v];
@@ -1739,6 +1817,89 @@ Status Engine::download(float* regrets, float* sums) {
       if (sums) std::memcpy(sums + nd.ref_offset + (size_t)a * n, sm.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 4);
     }
   }
+  return Status();
+}
+
+// Decision nodes in the reference's storage order (the device blocks are in
+// the same order, gpu_off_ increasing), cut into chunks of whole nodes of at
+// most STAGE_MAX elements; built on the first transfer.
+Status Engine::storage_chunks() {
+  if (!schunks_.empty() || g.storage_len == 0) return Status();
+  constexpr uint64_t STAGE_MAX = (uint64_t)1 << 26;
+  std::vector<uint32_t> players;
+  for (uint32_t v = 0; v < g.nodes.size(); v++)
+    if (g.nodes[v].kind == N_PLAYER) players.push_back(v);
+  std::sort(players.begin(), players.end(),
+            [&](uint32_t a, uint32_t b) { return g.nodes[a].ref_offset < g.nodes[b].ref_offset; });
+  std::vector<StorageBlockD> blk(players.size());
+  std::vector<StorageChunk> chunks;
+  StorageChunk c{0, 0, 0, 0};
+  uint64_t stage = 0;
+  for (size_t i = 0; i < players.size(); i++) {
+    const GNode& nd = g.nodes[players[i]];
+    const int q = nd.player;
+    const uint64_t len = (uint64_t)nd.nchild * (uint64_t)g.n[q];
+    if (c.count > 0 && c.len + len > STAGE_MAX) {
+      chunks.push_back(c);
+      c = StorageChunk{(uint32_t)i, 0, nd.ref_offset, 0};
+    }
+    if (c.count == 0) c = StorageChunk{(uint32_t)i, 0, nd.ref_offset, 0};
+    blk[i] = StorageBlockD{gpu_off_[players[i]], nd.ref_offset - c.host, nd.nchild, (uint32_t)g.n[q],
+                           (uint32_t)hp_[q], 0};
+    c.count++;
+    c.len += len;
+    stage = std::max(stage, c.len);
+  }
+  if (c.count > 0) chunks.push_back(c);
+  Status s;
+  if (!(s = dalloc(sblk_, blk.size(), "storage transfer table")).ok()) return s;
+  CK(cudaMemcpy(sblk_, blk.data(), blk.size() * sizeof(StorageBlockD), cudaMemcpyHostToDevice));
+  stage_len_ = stage;
+  schunks_ = std::move(chunks);
+  return Status();
+}
+
+namespace {
+// A device staging buffer freed on every return path.
+struct Staging {
+  void* p = nullptr;
+  ~Staging() {
+    if (p) cudaFree(p);
+  }
+};
+}  // namespace
+
+// Device storage (elements of elem_bytes) to the caller's reference-layout
+// array: per chunk, one pack launch and one copy to host memory.
+Status Engine::storage_out(const void* dev, void* host, int elem_bytes) {
+  Status s = storage_chunks();
+  if (!s.ok() || schunks_.empty()) return s;
+  Staging st;
+  CK(cudaMalloc(&st.p, stage_len_ * (uint64_t)elem_bytes));
+  for (const StorageChunk& c : schunks_) {
+    launch_storage_pack(elem_bytes, dev, st.p, sblk_ + c.first, (int)c.count, stream_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(static_cast<char*>(host) + c.host * elem_bytes, st.p, c.len * elem_bytes,
+                       cudaMemcpyDeviceToHost, stream_));
+  }
+  CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// The caller's reference-layout array to the device storage (padding
+// entries zeroed): per chunk, one copy from host memory and one unpack launch.
+Status Engine::storage_in(void* dev, const void* host, int elem_bytes) {
+  Status s = storage_chunks();
+  if (!s.ok() || schunks_.empty()) return s;
+  Staging st;
+  CK(cudaMalloc(&st.p, stage_len_ * (uint64_t)elem_bytes));
+  for (const StorageChunk& c : schunks_) {
+    CK(cudaMemcpyAsync(st.p, static_cast<const char*>(host) + c.host * elem_bytes, c.len * elem_bytes,
+                       cudaMemcpyHostToDevice, stream_));
+    launch_storage_unpack(elem_bytes, dev, st.p, sblk_ + c.first, (int)c.count, stream_);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(stream_));
   return Status();
 }
 
@@ -1759,42 +1920,23 @@ Status Engine::download_compressed_raw(std::vector<int16_t>& rq, std::vector<uin
 
 Status Engine::download_compressed(int16_t* regrets, uint16_t* sums, float* rscale, float* sscale) {
   if (!compressed_) return Status{DCFR_ERR_UNSUPPORTED, "the solver's storage is f32"};
-  std::vector<int16_t> rq;
-  std::vector<uint16_t> sq;
-  std::vector<float> rs, ss;
-  Status s = download_compressed_raw(rq, sq, rs, ss);
-  if (!s.ok()) return s;
-  for (uint32_t v = 0; v < g.nodes.size(); v++) {
-    const GNode& nd = g.nodes[v];
-    if (nd.kind != N_PLAYER) continue;
-    const int q = nd.player, n = g.n[q];
-    for (int a = 0; a < nd.nchild; a++) {
-      if (regrets)
-        std::memcpy(regrets + nd.ref_offset + (size_t)a * n, rq.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 2);
-      if (sums) std::memcpy(sums + nd.ref_offset + (size_t)a * n, sq.data() + gpu_off_[v] + (size_t)a * hp_[q], n * 2);
-    }
+  Status s;
+  if (regrets && !(s = storage_out(rq_, regrets, 2)).ok()) return s;
+  if (sums && !(s = storage_out(sq_, sums, 2)).ok()) return s;
+  if (g.player_nodes) {
+    if (rscale) CK(cudaMemcpyAsync(rscale, rscale_, (size_t)g.player_nodes * 4, cudaMemcpyDeviceToHost, stream_));
+    if (sscale) CK(cudaMemcpyAsync(sscale, sscale_, (size_t)g.player_nodes * 4, cudaMemcpyDeviceToHost, stream_));
   }
-  if (rscale) std::memcpy(rscale, rs.data(), (size_t)g.player_nodes * 4);
-  if (sscale) std::memcpy(sscale, ss.data(), (size_t)g.player_nodes * 4);
+  CK(cudaStreamSynchronize(stream_));
   return Status();
 }
 
 Status Engine::upload_compressed(const int16_t* regrets, const uint16_t* sums, const float* rscale,
                                  const float* sscale) {
   if (!compressed_) return Status{DCFR_ERR_UNSUPPORTED, "the solver's storage is f32"};
-  std::vector<int16_t> rq(gpu_len_, 0);
-  std::vector<uint16_t> sq(gpu_len_, 0);
-  for (uint32_t v = 0; v < g.nodes.size(); v++) {
-    const GNode& nd = g.nodes[v];
-    if (nd.kind != N_PLAYER) continue;
-    const int q = nd.player, n = g.n[q];
-    for (int a = 0; a < nd.nchild; a++) {
-      std::memcpy(rq.data() + gpu_off_[v] + (size_t)a * hp_[q], regrets + nd.ref_offset + (size_t)a * n, n * 2);
-      std::memcpy(sq.data() + gpu_off_[v] + (size_t)a * hp_[q], sums + nd.ref_offset + (size_t)a * n, n * 2);
-    }
-  }
-  CK(cudaMemcpyAsync(rq_, rq.data(), gpu_len_ * 2, cudaMemcpyHostToDevice, stream_));
-  CK(cudaMemcpyAsync(sq_, sq.data(), gpu_len_ * 2, cudaMemcpyHostToDevice, stream_));
+  Status s;
+  if (!(s = storage_in(rq_, regrets, 2)).ok()) return s;
+  if (!(s = storage_in(sq_, sums, 2)).ok()) return s;
   if (g.player_nodes) {
     CK(cudaMemcpyAsync(rscale_, rscale, (size_t)g.player_nodes * 4, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(sscale_, sscale, (size_t)g.player_nodes * 4, cudaMemcpyHostToDevice, stream_));
@@ -1805,20 +1947,9 @@ Status Engine::upload_compressed(const int16_t* regrets, const uint16_t* sums, c
 
 Status Engine::upload(const float* regrets, const float* sums) {
   if (compressed_) return Status{DCFR_ERR_UNSUPPORTED, "compressed storage: use dcfr_upload_storage_compressed"};
-  std::vector<float> r(gpu_len_, 0.0f), sm(gpu_len_, 0.0f);
-  for (uint32_t v = 0; v < g.nodes.size(); v++) {
-    const GNode& nd = g.nodes[v];
-    if (nd.kind != N_PLAYER) continue;
-    int q = nd.player, n = g.n[q];
-    for (int a = 0; a < nd.nchild; a++) {
-      std::memcpy(r.data() + gpu_off_[v] + (size_t)a * hp_[q], regrets + nd.ref_offset + (size_t)a * n, n * 4);
-      std::memcpy(sm.data() + gpu_off_[v] + (size_t)a * hp_[q], sums + nd.ref_offset + (size_t)a * n, n * 4);
-    }
-  }
-  CK(cudaMemcpyAsync(regrets_, r.data(), gpu_len_ * 4, cudaMemcpyHostToDevice, stream_));
-  CK(cudaMemcpyAsync(sums_, sm.data(), gpu_len_ * 4, cudaMemcpyHostToDevice, stream_));
-  CK(cudaStreamSynchronize(stream_));
-  return Status();
+  Status s;
+  if (!(s = storage_in(regrets_, regrets, 4)).ok()) return s;
+  return storage_in(sums_, sums, 4);
 }
 
 Status Engine::set_iterations(uint32_t t) {

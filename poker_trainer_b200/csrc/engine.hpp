@@ -73,6 +73,12 @@ void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
 void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
 void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
                             cudaStream_t s);
+// Storage blocks between the device layout and the reference's packed
+// layout; elem_bytes 4 (f32) or 2 (compressed storage).
+void launch_storage_pack(int elem_bytes, const void* dev, void* packed, const StorageBlockD* blocks, int nblocks,
+                         cudaStream_t s);
+void launch_storage_unpack(int elem_bytes, void* dev, const void* packed, const StorageBlockD* blocks, int nblocks,
+                           cudaStream_t s);
 
 // Status of a failed call: code + message.
 struct Status {
@@ -234,6 +240,18 @@ class Engine {
   float* sscale_ = nullptr;
   Status download_compressed_raw(std::vector<int16_t>& rq, std::vector<uint16_t>& sq, std::vector<float>& rs,
                                  std::vector<float>& ss);
+  // Transfers between the device storage and the reference layout, through
+  // a device staging buffer in chunks of whole decision nodes.
+  struct StorageChunk {
+    uint32_t first, count;  // blocks sblk_[first, first + count)
+    uint64_t host, len;     // elements [host, host + len) of the reference layout
+  };
+  std::vector<StorageChunk> schunks_;
+  StorageBlockD* sblk_ = nullptr;
+  uint64_t stage_len_ = 0;  // elements of the staging buffer (the largest chunk)
+  Status storage_chunks();
+  Status storage_out(const void* dev, void* host, int elem_bytes);
+  Status storage_in(void* dev, const void* host, int elem_bytes);
   float* reach_ = nullptr;
   float* vals_ = nullptr;
   uint32_t* alive_ = nullptr;

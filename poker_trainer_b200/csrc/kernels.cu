@@ -413,6 +413,60 @@ __global__ void traversal_start_kernel(uint32_t* __restrict__ alive, int nslots,
   pdl_launch_dependents();
 }
 
+// Storage blocks between the device layout (each action's row padded to hp
+// entries) and the reference's packed layout (rows of n entries): a block of
+// the grid per decision node, the elements copied as raw bits (f32 storage,
+// or the 16-bit values of compressed storage). Unpacking zeroes the padding.
+template <class T>
+__global__ void __launch_bounds__(256) storage_pack_kernel(const T* __restrict__ dev, T* __restrict__ packed,
+                                                            const StorageBlockD* __restrict__ blocks, int nblocks) {
+  for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const StorageBlockD B = blocks[b];
+    const uint32_t total = B.rows * B.n;
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+      const uint32_t a = i / B.n, h = i - a * B.n;
+      packed[B.host + i] = dev[B.dev + (uint64_t)a * B.hp + h];
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) storage_unpack_kernel(T* __restrict__ dev, const T* __restrict__ packed,
+                                                              const StorageBlockD* __restrict__ blocks, int nblocks) {
+  for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const StorageBlockD B = blocks[b];
+    const uint32_t total = B.rows * B.hp;
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+      const uint32_t a = i / B.hp, h = i - a * B.hp;
+      dev[B.dev + i] = h < B.n ? packed[B.host + (uint64_t)a * B.n + h] : T(0);
+    }
+  }
+}
+
+static int storage_grid(int nblocks) { return nblocks < 148 * 8 ? (nblocks > 0 ? nblocks : 1) : 148 * 8; }
+
+void launch_storage_pack(int elem_bytes, const void* dev, void* packed, const StorageBlockD* blocks, int nblocks,
+                         cudaStream_t s) {
+  if (nblocks <= 0) return;
+  if (elem_bytes == 4)
+    storage_pack_kernel<uint32_t><<<storage_grid(nblocks), 256, 0, s>>>(
+        static_cast<const uint32_t*>(dev), static_cast<uint32_t*>(packed), blocks, nblocks);
+  else
+    storage_pack_kernel<uint16_t><<<storage_grid(nblocks), 256, 0, s>>>(
+        static_cast<const uint16_t*>(dev), static_cast<uint16_t*>(packed), blocks, nblocks);
+}
+
+void launch_storage_unpack(int elem_bytes, void* dev, const void* packed, const StorageBlockD* blocks, int nblocks,
+                           cudaStream_t s) {
+  if (nblocks <= 0) return;
+  if (elem_bytes == 4)
+    storage_unpack_kernel<uint32_t><<<storage_grid(nblocks), 256, 0, s>>>(
+        static_cast<uint32_t*>(dev), static_cast<const uint32_t*>(packed), blocks, nblocks);
+  else
+    storage_unpack_kernel<uint16_t><<<storage_grid(nblocks), 256, 0, s>>>(
+        static_cast<uint16_t*>(dev), static_cast<const uint16_t*>(packed), blocks, nblocks);
+}
+
 void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
                             cudaStream_t s) {
   const int threads = 256, work = nslots > stride / 4 ? nslots : stride / 4;

@@ -115,6 +115,16 @@ struct DiscountD {
   int reach_weighted;
 };
 
+// One decision node's storage block for transfers to and from the
+// reference's layout (HostStorage, crates/solver/src/storage.rs): its
+// [rows][hp] block at element `dev` of the device storage, and its
+// [rows][n] block at element `host` of the reference layout, counted from
+// the start of the transfer chunk that holds it.
+struct StorageBlockD {
+  uint64_t dev, host;
+  uint32_t rows, n, hp, pad;
+};
+
 // Fast-precision terminal evaluation (terminal_fast.cu): one task per live
 // terminal; a showdown task also writes its paired fold's row.
 struct FastTask {

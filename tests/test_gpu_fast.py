@@ -158,7 +158,7 @@ def test_fast_workload_exploitability(gpu, spot):
     iterations, alpha 1.5 beta 0 gamma 2): exploitability within 1e-4
     relative of the oracle's after the same iterations."""
     cfg = workloads.river_spot() if spot == "river" else workloads.turn_spot()
-    iters = 1000 if spot == "river" else 200
+    iters = 1000
     o = OracleSolver(cfg)
     g = Solver.new(cfg)
     o.iterate(iters)
