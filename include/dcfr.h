@@ -316,7 +316,12 @@ int dcfr_ranges_after(dcfr_solver* s, const dcfr_step* path, size_t n, float out
  * regrets and len f32 strategy sums. Used to resume a solve elsewhere
  * (lib.rs:532-540) and by the parity tests. A solver with compressed
  * storage downloads its values decoded (load_regrets / load_strat,
- * storage.rs:226-268) and uploads only through the compressed call. */
+ * storage.rs:226-268) and uploads only through the compressed call. The
+ * f32 and compressed transfers remove (or restore) the device layout's
+ * padding on the device and copy each chunk (at most 64 M values) straight
+ * between the device and the caller's arrays; page-locked arrays
+ * (cudaHostAlloc) take the fastest copies. A transfer allocates a device
+ * staging buffer of up to 256 MB for its duration. */
 int dcfr_storage_len(const dcfr_solver* s, uint64_t* len);
 int dcfr_download_storage(dcfr_solver* s, float* regrets, float* sums, uint64_t len);
 int dcfr_upload_storage(dcfr_solver* s, const float* regrets, const float* sums, uint64_t len);
@@ -373,10 +378,11 @@ typedef struct dcfr_kernel_profile {
  * device time of the last dcfr_solve in milliseconds (CUDA events on the
  * handle's stream at its start and end). dcfr_setup_profile: where the
  * handle's setup went, host wall clock in milliseconds: the game (tree,
- * hands, isomorphism) built on the host; device storage, hands and chance
- * tables allocated and uploaded; strength tables and terminal layouts
- * built on the device; both traversal plans built and uploaded; reach and
- * value rows allocated; all of dcfr_create; and, when they happen, the
+ * hands, isomorphism) built on the host; hands and chance tables uploaded;
+ * strength tables and terminal layouts built on the device; both traversal
+ * plans built (on two host threads while the storage is allocated and
+ * cleared on the device) and uploaded; reach and value rows allocated; all
+ * of dcfr_create; and, when they happen, the
  * iteration graph's capture (first dcfr_iterate / dcfr_solve) and the
  * best-response and average graphs' (first exploitability or root values). */
 typedef struct dcfr_setup_profile {

@@ -433,11 +433,7 @@ Status Batch::Impl::init(const dcfr_config* cfgs, int count) {
     max_stride = std::max(max_stride, stride);
     const size_t N = g.nodes.size();
     // Storage: player blocks [a][hp_q] in the reference's node order.
-    std::vector<uint32_t> players;
-    for (uint32_t v = 0; v < N; v++)
-      if (g.nodes[v].kind == N_PLAYER) players.push_back(v);
-    std::sort(players.begin(), players.end(),
-              [&](uint32_t a, uint32_t b) { return g.nodes[a].ref_offset < g.nodes[b].ref_offset; });
+    const std::vector<uint32_t> players = players_in_storage_order(g);
     node_off[i].assign(N, 0);
     uint64_t len = 0;
     for (uint32_t v : players) {

@@ -257,11 +257,7 @@ Status Engine::init() {
 
   // Storage layout: one [actions][hp_q] block per decision node, in the
   // reference's node order (Node::offset, tree.rs:462, 468).
-  std::vector<uint32_t> players;
-  for (uint32_t v = 0; v < N; v++)
-    if (g.nodes[v].kind == N_PLAYER) players.push_back(v);
-  std::sort(players.begin(), players.end(),
-            [&](uint32_t a, uint32_t b) { return g.nodes[a].ref_offset < g.nodes[b].ref_offset; });
+  const std::vector<uint32_t> players = players_in_storage_order(g);
   gpu_off_.assign(N, 0);
   gpu_len_ = 0;
   for (uint32_t v : players) {
@@ -270,24 +266,6 @@ Status Engine::init() {
   }
   Status s;
   compressed_ = g.compressed;
-  if (compressed_) {
-    // Storage::Compressed (storage.rs:92-97): 16-bit values, a scale of
-    // each kind per decision node (its ordinal, the reference's slot).
-    const size_t slots = std::max<size_t>(g.player_nodes, 1);
-    if (!(s = dalloc(rq_, gpu_len_, "storage")).ok()) return s;
-    if (!(s = dalloc(sq_, gpu_len_, "storage")).ok()) return s;
-    if (!(s = dalloc(rscale_, slots, "storage scales")).ok()) return s;
-    if (!(s = dalloc(sscale_, slots, "storage scales")).ok()) return s;
-    CK(cudaMemsetAsync(rq_, 0, gpu_len_ * 2, stream_));
-    CK(cudaMemsetAsync(sq_, 0, gpu_len_ * 2, stream_));
-    CK(cudaMemsetAsync(rscale_, 0, slots * 4, stream_));
-    CK(cudaMemsetAsync(sscale_, 0, slots * 4, stream_));
-  } else {
-    if (!(s = dalloc(regrets_, gpu_len_, "storage")).ok()) return s;
-    if (!(s = dalloc(sums_, gpu_len_, "storage")).ok()) return s;
-    CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
-    CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
-  }
 
   tstride_ = std::max(g.n[0], g.n[1]);
   pstride_ = (2 * tstride_ + TERM_CHUNK - 1) / TERM_CHUNK * TERM_CHUNK;
@@ -373,14 +351,18 @@ Status Engine::init() {
     if (fast_ && !(s = ensure_fast_layouts()).ok()) return s;
   }
   phase(setup.tables_ms);
-  // Plans for the two traversals of an iteration, built concurrently on two
-  // host threads (build_plan only reads the game and the engine's layouts).
+  // Plans for the two traversals of an iteration, built on two host threads
+  // (build_plan only reads the game and host-side fields of the engine)
+  // while this thread allocates and clears the storage on the device.
   {
     Status ps[2];
     for (int p = 0; p < 2; p++) full_[p].reset(new Plan());
-    std::thread other([&]() { ps[1] = build_plan(0, 1, *full_[1]); });
-    ps[0] = build_plan(0, 0, *full_[0]);
-    other.join();
+    std::thread t1([&]() { ps[1] = build_plan(0, 1, *full_[1]); });
+    std::thread t0([&]() { ps[0] = build_plan(0, 0, *full_[0]); });
+    const Status sa = alloc_storage();
+    t0.join();
+    t1.join();
+    if (!sa.ok()) return sa;
     for (int p = 0; p < 2; p++) {
       if (!ps[p].ok()) return ps[p];
       max_slots_ = std::max<uint64_t>(max_slots_, full_[p]->nslots);
@@ -434,6 +416,31 @@ Status Engine::init() {
   CK(cudaMemsetAsync(counter_, 0, 4, stream_));
   if (!(s = ensure_discounts(1024)).ok()) return s;
   CK(cudaStreamSynchronize(stream_));
+  return Status();
+}
+
+// Storage in the layout of Engine::init, zeroed: f32 regrets and strategy
+// sums, or 16-bit values with a scale of each kind per decision node.
+Status Engine::alloc_storage() {
+  Status s;
+  if (compressed_) {
+    // Storage::Compressed (storage.rs:92-97): 16-bit values, a scale of
+    // each kind per decision node (its ordinal, the reference's slot).
+    const size_t slots = std::max<size_t>(g.player_nodes, 1);
+    if (!(s = dalloc(rq_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(sq_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(rscale_, slots, "storage scales")).ok()) return s;
+    if (!(s = dalloc(sscale_, slots, "storage scales")).ok()) return s;
+    CK(cudaMemsetAsync(rq_, 0, gpu_len_ * 2, stream_));
+    CK(cudaMemsetAsync(sq_, 0, gpu_len_ * 2, stream_));
+    CK(cudaMemsetAsync(rscale_, 0, slots * 4, stream_));
+    CK(cudaMemsetAsync(sscale_, 0, slots * 4, stream_));
+  } else {
+    if (!(s = dalloc(regrets_, gpu_len_, "storage")).ok()) return s;
+    if (!(s = dalloc(sums_, gpu_len_, "storage")).ok()) return s;
+    CK(cudaMemsetAsync(regrets_, 0, gpu_len_ * 4, stream_));
+    CK(cudaMemsetAsync(sums_, 0, gpu_len_ * 4, stream_));
+  }
   return Status();
 }
 
@@ -1826,11 +1833,7 @@ Status Engine::download(float* regrets, float* sums) {
 Status Engine::storage_chunks() {
   if (!schunks_.empty() || g.storage_len == 0) return Status();
   constexpr uint64_t STAGE_MAX = (uint64_t)1 << 26;
-  std::vector<uint32_t> players;
-  for (uint32_t v = 0; v < g.nodes.size(); v++)
-    if (g.nodes[v].kind == N_PLAYER) players.push_back(v);
-  std::sort(players.begin(), players.end(),
-            [&](uint32_t a, uint32_t b) { return g.nodes[a].ref_offset < g.nodes[b].ref_offset; });
+  const std::vector<uint32_t> players = players_in_storage_order(g);
   std::vector<StorageBlockD> blk(players.size());
   std::vector<StorageChunk> chunks;
   StorageChunk c{0, 0, 0, 0};

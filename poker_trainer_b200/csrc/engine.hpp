@@ -339,6 +339,7 @@ class Engine {
   int iter_kernels_ = 0, pair_kernels_ = 0;
 
   Status init();
+  Status alloc_storage();
   Status build_plan(uint32_t root, int p, Plan& plan);
   Status upload_plan(Plan& plan);
   void row_args(int p, RowArgs& A) const;

@@ -537,6 +537,13 @@ static void build_iso(Game& g) {
   }
 }
 
+std::vector<uint32_t> players_in_storage_order(const Game& g) {
+  std::vector<uint32_t> players((size_t)g.player_nodes);
+  for (uint32_t v = 0; v < (uint32_t)g.nodes.size(); v++)
+    if (g.nodes[v].kind == N_PLAYER) players[g.nodes[v].index] = v;
+  return players;
+}
+
 void normalize_rows(float* s, int na, int n) {
   for (int h = 0; h < n; h++) {
     float d = s[h];

@@ -113,5 +113,9 @@ std::vector<Act> state_actions(const Betting& st, const dcfr_menu& menu, int64_t
 // side, for the path walk of queries.
 void normalize_rows(float* s, int na, int n);
 
+// Decision nodes in the reference's storage order (Node::offset). build_game
+// gives each decision node its ordinal (`index`) and its storage offset at
+// the same step, so the ordinal orders them: no sort needed.
+std::vector<uint32_t> players_in_storage_order(const Game& g);
 
 }  // namespace dcfr
