@@ -1202,9 +1202,10 @@ void Engine::fast_args(int p, FastArgs& A) const {
 
 // Enqueues one traversal: liveness reset, root row, down levels, terminals,
 // up levels (deepest first); the root's value row is copied to root_out.
-void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out) {
+void Engine::enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out, bool advance) {
   const int p = plan.p, o = p ^ 1;
-  launch_traversal_start(alive_, (int)plan.nslots, reach_, root_row, stride_, stream_);
+  launch_traversal_start(alive_, (int)plan.nslots, reach_, root_row, stride_, advance ? counter_ : nullptr,
+                         disc_table_, disc_len_, cur_disc_, stream_);
   mark(DCFR_KERNEL_OTHER);
   RowArgs A;
   row_args(p, A);
@@ -1418,14 +1419,14 @@ Status Engine::capture_graphs() {
   cudaGraph_t graph;
   // One DCFR iteration: t += 1, then player 0's and player 1's traversals
   // with the same discounts (lib.rs:577-585).
+  // The first traversal's start kernel advances the iteration.
   CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-  launch_advance(counter_, disc_table_, disc_len_, cur_disc_, stream_);
-  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr);
+  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr, true);
   enqueue_traversal(*full_[1], M_CFR, root_rows_ + stride_, nullptr);
   CK(cudaStreamEndCapture(stream_, &graph));
   CK(cudaGraphInstantiate(&iter_graph_, graph, 0));
   cudaGraphDestroy(graph);
-  iter_kernels_ = 1 + full_[0]->kernels + full_[1]->kernels;
+  iter_kernels_ = full_[0]->kernels + full_[1]->kernels;
   setup.iteration_graph_ms += ms_since(t0);
   return Status();
 }
@@ -1476,8 +1477,7 @@ Status Engine::capture_profiled_graph() {
   marking_ = &marks_;
   CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
   mark(-1);
-  launch_advance(counter_, disc_table_, disc_len_, cur_disc_, stream_);
-  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr);
+  enqueue_traversal(*full_[0], M_CFR, root_rows_, nullptr, true);
   enqueue_traversal(*full_[1], M_CFR, root_rows_ + stride_, nullptr);
   marking_ = nullptr;
   cudaError_t e = cudaStreamEndCapture(stream_, &prof_graph_);
@@ -1528,7 +1528,6 @@ Status Engine::iterate_profiled(uint32_t n, dcfr_kernel_profile& out) {
     out.launches[c] = (uint64_t)n * (full_[0]->class_kernels[c] + full_[1]->class_kernels[c]);
     out.bytes[c] = (double)n * (full_[0]->class_bytes[c] + full_[1]->class_bytes[c]);
   }
-  out.launches[DCFR_KERNEL_OTHER] += n;  // the discount advance
   return Status();
 }
 

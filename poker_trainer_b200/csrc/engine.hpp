@@ -70,8 +70,10 @@ int fast_emax(int tstride);
 int fast_blocks_per_sm(int stride, int emax, int cstride, int tstride);
 void launch_evaluate(const unsigned long long* masks, uint32_t* out, int n, cudaStream_t s);
 void launch_five_card_counts(unsigned long long* counts, cudaStream_t s);
-void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s);
+// counter non-null: also advance the DCFR iteration (t += 1, the discounts
+// of iteration t from the table into cur).
 void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
+                            uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur,
                             cudaStream_t s);
 // Storage blocks between the device layout and the reference's packed
 // layout; elem_bytes 4 (f32) or 2 (compressed storage).
@@ -345,7 +347,7 @@ class Engine {
   void row_args(int p, RowArgs& A) const;
   void term_args(int p, TermArgs& A) const;
   void fast_args(int p, FastArgs& A) const;
-  void enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out);
+  void enqueue_traversal(const Plan& plan, int mode, const float* root_row, float* root_out, bool advance = false);
   Status ensure_discounts(uint32_t max_t);
   Status capture_graphs();
   Status capture_eval_graphs();

@@ -254,13 +254,6 @@ __global__ void five_card_counts_kernel(unsigned long long* counts) {
   if (threadIdx.x < 9) atomicAdd(&counts[threadIdx.x], (unsigned long long)local[threadIdx.x]);
 }
 
-// Iteration counter: t += 1 and the iteration's discounts from the table.
-__global__ void advance_kernel(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur) {
-  uint32_t t = *counter + 1;
-  *counter = t;
-  *cur = table[t < table_len ? t : table_len - 1];
-}
-
 // ---------------------------------------------------------- host launchers
 // One block per node (and chunk of 4 * ROW_MAX_THREADS hands): a thread per 4
 // hands, whole warps. Launched with programmatic stream serialization so the
@@ -394,18 +387,24 @@ void launch_five_card_counts(unsigned long long* counts, cudaStream_t s) {
   five_card_counts_kernel<<<52 * 51 / 2, 256, 0, s>>>(counts);
 }
 
-void launch_advance(uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur, cudaStream_t s) {
-  advance_kernel<<<1, 1, 0, s>>>(counter, table, table_len, cur);
-}
 
 // Start of a traversal: every liveness flag cleared but the root slot's, and
 // the root's reach row copied into slot 0. One launch in place of two
 // memsets and a copy, chained to the traversal's level launches by
 // programmatic dependent launch (the flags are cleared only once the
-// previous traversal's kernels, which read them, are complete).
+// previous traversal's kernels, which read them, are complete). The first
+// traversal of a DCFR iteration also advances the iteration (counter given):
+// t += 1 and the iteration's discounts from the table, read by the
+// traversal's row kernels after their wait.
 __global__ void traversal_start_kernel(uint32_t* __restrict__ alive, int nslots, float* __restrict__ reach,
-                                       const float* __restrict__ root_row, int stride) {
+                                       const float* __restrict__ root_row, int stride, uint32_t* counter,
+                                       const DiscountD* table, uint32_t table_len, DiscountD* cur) {
   pdl_wait();
+  if (counter && blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t t = *counter + 1;
+    *counter = t;
+    *cur = table[t < table_len ? t : table_len - 1];
+  }
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x, step = gridDim.x * blockDim.x;
   for (int i = i0; i < nslots; i += step) alive[i] = i == 0 ? 1u : 0u;
   for (int i = i0; i < stride / 4; i += step)
@@ -468,6 +467,7 @@ void launch_storage_unpack(int elem_bytes, void* dev, const void* packed, const 
 }
 
 void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const float* root_row, int stride,
+                            uint32_t* counter, const DiscountD* table, uint32_t table_len, DiscountD* cur,
                             cudaStream_t s) {
   const int threads = 256, work = nslots > stride / 4 ? nslots : stride / 4;
   int blocks = (work + threads - 1) / threads;
@@ -483,7 +483,8 @@ void launch_traversal_start(uint32_t* alive, int nslots, float* reach, const flo
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, traversal_start_kernel, alive, nslots, reach, root_row, stride);
+  cudaLaunchKernelEx(&cfg, traversal_start_kernel, alive, nslots, reach, root_row, stride, counter, table, table_len,
+                     cur);
 }
 
 }  // namespace dcfr
