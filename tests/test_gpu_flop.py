@@ -10,7 +10,9 @@ standards (crates/solver/src/gpu/engine/tests.rs):
   tests.rs:481-490; fast_converged_solves_match_cpu, tests.rs:492-512);
 - exact precision bit for bit: two iterations reproduce the oracle's
   committed exploitability, root values and storage digest
-  (exact_solves_match_cpu_bit_for_bit, tests.rs:729-754).
+  (exact_solves_match_cpu_bit_for_bit, tests.rs:729-754); that storage
+  uploaded into a fresh solver downloads with the same digest (the chunked
+  transfers in both directions).
 
 The flop tree holds about 2.5 G storage cells (20 GB of regrets and strategy
 sums in each solver); the oracle runs its chance children on all host
@@ -50,6 +52,16 @@ def test_flop_exact_matches_fixture(gpu):
     assert float(g.exploitability()).hex() == f["exploitability"]
     assert [float(v).hex() for v in g.root_values()] == f["root_values"]
     r, s = g.download_storage()
+    g.close()
+    assert storage_digest(r, s) == f["storage_sha256"]
+    # The same storage up into a fresh solver (all zeros) and down again:
+    # both transfers cross in about 40 chunks of at most 64 M values, so a
+    # chunk that went astray shows as zeros or misplaced values.
+    g = Solver.new(cfg)
+    g.upload_storage(r, s)
+    r[:] = 0.0
+    s[:] = 0.0
+    g.download_storage(out=(r, s))
     g.close()
     assert storage_digest(r, s) == f["storage_sha256"]
 
